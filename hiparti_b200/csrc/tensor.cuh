@@ -1,0 +1,83 @@
+// tensor.cuh -- the device-resident tensor behind a ptiB200Tensor handle.
+#pragma once
+#include "common.cuh"
+
+#include <array>
+#include <memory>
+
+namespace pti {
+
+constexpr int kMaxModes = 8;
+
+// Per-mode schedule of a HiCOO tensor: the blocks re-ordered by their block
+// coordinate in the output mode (a materialised form of the reference's
+// per-mode kernel scheduler kschr, src/sptensor/hicoo/convert.c:378-421), with
+// the nonzeros of each block re-ordered by their in-block output offset.  The
+// arrays use the HiCOO layout (bptr / binds / einds / values) so the same
+// kernels read them; `tiles` splits the nonzeros into nnz-balanced work items
+// that never split a block row's tile flush incorrectly (see mttkrp.cu).
+struct HicooModePlan {
+    bool ready = false;
+    uint64_t nb = 0;
+    DevBuf bptr;                          // uint64 [nb+1]
+    std::array<DevBuf, kMaxModes> binds;  // uint32 [nb]
+    std::array<DevBuf, kMaxModes> einds;  // uint8  [nnz]
+    DevBuf vals;                          // float  [nnz]
+    DevBuf tile_block;                    // uint32 [ntiles+1]: first block of each tile
+    uint32_t ntiles = 0;
+};
+
+// Per-mode schedule of a COO tensor: nonzeros sorted by the output-mode index.
+struct CooModePlan {
+    bool ready = false;
+    std::array<DevBuf, kMaxModes> inds;   // uint32 [nnz]
+    DevBuf vals;                          // float [nnz]
+};
+
+}  // namespace pti
+
+struct ptiB200Tensor {
+    bool hicoo = false;
+    uint32_t nmodes = 0;
+    std::vector<uint32_t> ndims;
+    uint64_t nnz = 0;
+    int device = 0;
+
+    // COO storage (also kept for HiCOO tensors built on the device from COO)
+    std::array<pti::DevBuf, pti::kMaxModes> inds;  // uint32 [nnz]
+    pti::DevBuf vals;                              // float  [nnz]
+
+    // HiCOO storage
+    uint64_t nb = 0;
+    uint8_t sb = 0, sk = 0, sc = 0;
+    pti::DevBuf bptr;                                // uint64 [nb+1]
+    std::array<pti::DevBuf, pti::kMaxModes> binds;   // uint32 [nb]
+    std::array<pti::DevBuf, pti::kMaxModes> einds;   // uint8  [nnz]
+    pti::DevBuf tile_block;                          // first block of each nnz tile
+    uint32_t ntiles = 0;
+
+    std::array<pti::CooModePlan, pti::kMaxModes> coo_plan;
+    std::array<pti::HicooModePlan, pti::kMaxModes> hicoo_plan;
+};
+
+namespace pti {
+
+// Allocation sizes are rounded up to 64 bytes plus one 64-byte guard so that
+// vectorised and bulk copies of a final partial tile stay inside the buffer.
+inline size_t padded(size_t bytes) { return ((bytes + 63) / 64) * 64 + 64; }
+
+int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
+int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s);
+
+// MTTKRP launchers; factors are device pointers (element type ft), out is FP32.
+int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
+                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
+int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s);
+
+// Host-struct MTTKRP used by the reference entry points.
+int mttkrp_host_coo(const ptiSparseTensor *X, ptiMatrix **mats, const ptiIndex *mats_order,
+                    ptiIndex mode);
+int mttkrp_host_hicoo(const ptiSparseTensorHiCOO *H, ptiMatrix **mats, const ptiIndex *mats_order,
+                      ptiIndex mode);
+
+}  // namespace pti

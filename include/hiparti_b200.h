@@ -1,0 +1,287 @@
+/*
+ * hiparti_b200.h -- C ABI of the B200 (sm_100a) implementation of HiParTI's
+ * sparse MTTKRP / CPD-ALS path.
+ *
+ * The types, struct layouts and function signatures below are byte- and
+ * call-compatible with the reference headers, so a C program written against
+ * HiParTI's MTTKRP/CPD entry points links against libhiparti_b200.so instead of
+ * libHiParTI.so without source changes.  Every reference entry point declared
+ * here runs its arithmetic on the GPU; there is no CPU fallback.  Functions
+ * whose names start with ptiB200 are extensions with no reference counterpart:
+ * they keep tensors and factor matrices resident in device memory.
+ *
+ * Citations are to files of the reference project (pnnl/HiParTI).
+ */
+#ifndef HIPARTI_B200_H
+#define HIPARTI_B200_H
+
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Scalar types: include/includes/types.h:27-98 (32-bit indices, FP32 values,
+ * 8-bit element indices, 64-bit nonzero counters).
+ * ------------------------------------------------------------------------ */
+typedef uint32_t ptiIndex;
+typedef uint32_t ptiBlockIndex;
+typedef float    ptiValue;
+typedef uint8_t  ptiElementIndex;
+typedef uint16_t ptiBlockMatrixIndex;
+typedef ptiBlockIndex ptiBlockNnzIndex;
+typedef uint64_t ptiNnzIndex;
+
+/* Error codes: include/includes/macros.h:47-56. */
+typedef enum {
+    PTIERR_NO_ERROR       = 0,
+    PTIERR_UNKNOWN        = 1,
+    PTIERR_SHAPE_MISMATCH = 2,
+    PTIERR_VALUE_ERROR    = 3,
+    PTIERR_ZERO_DIVISION  = 4,
+    PTIERR_NO_MORE        = 99,
+    PTIERR_OS_ERROR       = 0x10000,
+    PTIERR_CUDA_ERROR     = 0x20000
+} PtiError;
+
+/* ---------------------------------------------------------------------------
+ * Containers: include/includes/structs.h:27-56 (vectors), :64-82 (matrices),
+ * :142-149 (COO tensor), :155-185 (HiCOO tensor), :254-271 (Kruskal tensors).
+ * ------------------------------------------------------------------------ */
+typedef struct { ptiNnzIndex len; ptiNnzIndex cap; ptiValue        *data; } ptiValueVector;
+typedef struct { ptiNnzIndex len; ptiNnzIndex cap; ptiIndex        *data; } ptiIndexVector;
+typedef struct { ptiNnzIndex len; ptiNnzIndex cap; ptiElementIndex *data; } ptiElementIndexVector;
+typedef struct { ptiNnzIndex len; ptiNnzIndex cap; ptiBlockIndex   *data; } ptiBlockIndexVector;
+typedef struct { ptiNnzIndex len; ptiNnzIndex cap; ptiNnzIndex     *data; } ptiNnzIndexVector;
+
+/* Row-major dense matrix; stride = ncols rounded up to a multiple of 8. */
+typedef struct {
+    ptiIndex nrows;
+    ptiIndex ncols;
+    ptiIndex cap;
+    ptiIndex stride;
+    ptiValue *values;
+} ptiMatrix;
+
+/* Dense matrix with a small rank (ncols and stride are 8-bit). */
+typedef struct {
+    ptiIndex        nrows;
+    ptiElementIndex ncols;
+    ptiIndex        cap;
+    ptiElementIndex stride;
+    ptiValue        *values;
+} ptiRankMatrix;
+
+/* Coordinate (COO) sparse tensor, indices stored per mode. */
+typedef struct {
+    ptiIndex nmodes;
+    ptiIndex *sortorder;
+    ptiIndex *ndims;
+    ptiNnzIndex nnz;
+    ptiIndexVector *inds;
+    ptiValueVector values;
+} ptiSparseTensor;
+
+/* Hierarchical COO (HiCOO) sparse tensor. */
+typedef struct {
+    ptiIndex    nmodes;
+    ptiIndex    *sortorder;
+    ptiIndex    *ndims;
+    ptiNnzIndex nnz;
+    ptiElementIndex sb_bits;      /* block edge = 2^sb_bits            */
+    ptiElementIndex sk_bits;      /* kernel (super-block) edge = 2^sk  */
+    ptiElementIndex sc_bits;      /* chunk size in nonzeros = 2^sc     */
+    ptiNnzIndexVector kptr;       /* first block of each kernel, + nb  */
+    ptiIndexVector  **kschr;      /* [mode][kernel row] -> kernel ids  */
+    ptiIndex        *nkiters;     /* [mode] longest kschr list         */
+    ptiNnzIndexVector cptr;       /* chunk pointers over blocks        */
+    ptiIndexVector  **kschr_balanced;
+    ptiIndexVector  **kschr_balanced_pos;
+    ptiIndex        *nkpars;
+    ptiIndexVector  *kschr_rest;
+    ptiNnzIndexVector knnzs;      /* nonzeros of each kernel           */
+    ptiNnzIndexVector bptr;       /* nb+1 nonzero offsets of blocks    */
+    ptiBlockIndexVector   *binds; /* [mode] block coordinates, nb each */
+    ptiElementIndexVector *einds; /* [mode] in-block offsets, nnz each */
+    ptiValueVector values;
+} ptiSparseTensorHiCOO;
+
+typedef struct {
+    ptiIndex nmodes;
+    ptiIndex rank;
+    ptiIndex *ndims;
+    ptiValue *lambda;
+    double fit;
+    ptiMatrix **factors;
+} ptiKruskalTensor;
+
+typedef struct {
+    ptiIndex nmodes;
+    ptiElementIndex rank;
+    ptiIndex *ndims;
+    ptiValue *lambda;
+    double fit;
+    ptiRankMatrix **factors;
+} ptiRankKruskalTensor;
+
+/* ---------------------------------------------------------------------------
+ * Error reporting: include/includes/helper_funcs.h:29-30,39-40.
+ * A failing call records (module, file, line, reason) in a thread-local slot
+ * and returns the code; ptiGetLastError returns that code and the strings.
+ * ------------------------------------------------------------------------ */
+int  ptiGetLastError(const char **module, const char **file, unsigned *line, const char **reason);
+void ptiClearLastError(void);
+int  ptiCudaSetDevice(int device);
+int  ptiCudaGetLastError(void);
+
+/* ---------------------------------------------------------------------------
+ * Container life cycle.
+ * ------------------------------------------------------------------------ */
+/* include/includes/sptensors.h:23-25 */
+int  ptiNewSparseTensor(ptiSparseTensor *tsr, ptiIndex nmodes, const ptiIndex ndims[]);
+void ptiFreeSparseTensor(ptiSparseTensor *tsr);
+/* include/includes/sptensors.h:26 (sum of squared values, FP64 accumulation; GPU) */
+double SparseTensorFrobeniusNormSquared(ptiSparseTensor const * const ptien);
+/* include/includes/sptensors.h:27 -- text .tns (header "N\nI_0 ... I_{N-1}")
+ * or SPLATT .bin, selected by file extension as in src/sptensor/load.c:277-297 */
+int  ptiLoadSparseTensor(ptiSparseTensor *tsr, ptiIndex start_index, char const * const fname);
+
+/* include/includes/matrices.h:26-34 */
+int  ptiNewMatrix(ptiMatrix *mtx, ptiIndex const nrows, ptiIndex const ncols);
+int  ptiRandomizeMatrix(ptiMatrix *mtx);           /* A[i,j] = i+j+1, src/matrix/matrix.c:67-74 */
+int  ptiConstantMatrix(ptiMatrix * const mtx, ptiValue const val);
+void ptiFreeMatrix(ptiMatrix *mtx);
+
+/* include/includes/ktensors.h:23-25 */
+int  ptiNewKruskalTensor(ptiKruskalTensor *ktsr, ptiIndex nmodes, const ptiIndex ndims[], ptiIndex rank);
+void ptiFreeKruskalTensor(ptiKruskalTensor *ktsr);
+int  ptiNewRankKruskalTensor(ptiRankKruskalTensor *ktsr, ptiIndex nmodes, const ptiIndex ndims[], ptiElementIndex rank);
+void ptiFreeRankKruskalTensor(ptiRankKruskalTensor *ktsr);
+/* include/includes/matrices.h:66,73 */
+int  ptiNewRankMatrix(ptiRankMatrix *mtx, ptiIndex const nrows, ptiElementIndex const ncols);
+void ptiFreeRankMatrix(ptiRankMatrix *mtx);
+
+/* include/includes/sptensors.h:104-119 */
+int  ptiNewSparseTensorHiCOO(ptiSparseTensorHiCOO *hitsr, const ptiIndex nmodes, const ptiIndex ndims[],
+                             const ptiNnzIndex nnz, const ptiElementIndex sb_bits,
+                             const ptiElementIndex sk_bits, const ptiElementIndex sc_bits);
+void ptiFreeSparseTensorHiCOO(ptiSparseTensorHiCOO *hitsr);
+
+/* include/includes/sptensors.h:120-127, src/sptensor/hicoo/convert.c:646-860.
+ * COO -> HiCOO on the GPU.  Output arrays are bit-identical to the reference
+ * for tensors with unique coordinates (3-D: coordinates < 2^24; 4-D: any);
+ * as in the reference, the caller's COO tensor is left sorted in HiCOO order
+ * (kernels row-major, nonzeros in Morton order inside each kernel).  tk is
+ * accepted and ignored.  Only 3-D and 4-D tensors are supported, as in
+ * src/sptensor/sort.c:414-430. */
+int  ptiSparseTensorToHiCOO(ptiSparseTensorHiCOO *hitsr, ptiNnzIndex *max_nnzb, ptiSparseTensor *tsr,
+                            const ptiElementIndex sb_bits, const ptiElementIndex sk_bits,
+                            const ptiElementIndex sc_bits, int const tk);
+
+/* ---------------------------------------------------------------------------
+ * MTTKRP.  mats[0..N-1] are the factor matrices (row i of mats[k] is the rank-R
+ * row of index i in mode k); mats[N] receives the result for `mode`
+ * (mats[mode]->nrows rows of stride floats; rows are overwritten, pad columns
+ * are zeroed).  mats_order[1..N-1] lists the modes multiplied together.
+ * All entry points below run on the current CUDA device, copy the host
+ * arguments in, and return once mats[N] has been written back.
+ * ------------------------------------------------------------------------ */
+/* include/includes/sptensors.h:179-183, src/sptensor/mttkrp.c:39-163 */
+int ptiMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex const mats_order[],
+              ptiIndex const mode);
+/* include/includes/sptensors.h:184-189 (tk ignored) */
+int ptiOmpMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex const mats_order[],
+                 ptiIndex const mode, const int tk);
+/* include/includes/sptensors.h:190-196 (copy_mats unused; tk ignored) */
+int ptiOmpMTTKRP_Reduce(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiMatrix * copy_mats[],
+                        ptiIndex const mats_order[], ptiIndex const mode, const int tk);
+/* include/includes/sptensors.h:204-215, src/sptensor/mttkrp_cuda.cu:41-374 and
+ * src/sptensor/mttkrp_cuda_onekernel.cu:41-426 (impl_num ignored; any order N). */
+int ptiCudaMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex * const mats_order,
+                  ptiIndex const mode, ptiIndex const impl_num);
+int ptiCudaMTTKRPOneKernel(ptiSparseTensor const * const X, ptiMatrix ** const mats,
+                           ptiIndex * const mats_order, ptiIndex const mode, ptiIndex const impl_num);
+
+/* include/includes/sptensors.h:253-257, src/sptensor/hicoo/mttkrp.c:61-310 */
+int ptiMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix * mats[],
+                   ptiIndex const mats_order[], ptiIndex const mode);
+/* include/includes/sptensors.h:263-269 (tk, tb ignored) */
+int ptiOmpMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix * mats[],
+                      ptiIndex const mats_order[], ptiIndex const mode, const int tk, const int tb);
+/* include/includes/sptensors.h:302-308, src/sptensor/hicoo/mttkrp_cuda.cu:41-265
+ * (max_nnzb and impl_num ignored: no limit on nonzeros per block; any order N). */
+int ptiCudaMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix ** const mats,
+                       ptiIndex * const mats_order, ptiIndex const mode, ptiNnzIndex const max_nnzb,
+                       int const impl_num);
+
+/* ---------------------------------------------------------------------------
+ * CPD-ALS: include/includes/cpds.h:26-57, src/sptensor/cpd.c:32-208.
+ * The ALS loop runs on the GPU in FP32 factors with FP64 Gram matrices,
+ * Cholesky solve and fit.  Factors start from ptiRandomizeMatrix (i+j+1) as in
+ * src/sptensor/cpd.c:181-187.  ktensor->lambda must come from
+ * ptiNewKruskalTensor; ktensor->factors is allocated here (N+1 pointers,
+ * factors[N] released) as in src/sptensor/cpd.c:200-205.
+ * ------------------------------------------------------------------------ */
+int ptiCpdAls(ptiSparseTensor const * const ptien, ptiIndex const rank, ptiIndex const niters,
+              double const tol, ptiKruskalTensor * ktensor);
+int ptiOmpCpdAls(ptiSparseTensor const * const ptien, ptiIndex const rank, ptiIndex const niters,
+                 double const tol, const int tk, const int use_reduce, ptiKruskalTensor * ktensor);
+int ptiCudaCpdAls(ptiSparseTensor const * const ptien, ptiIndex const rank, ptiIndex const niters,
+                  double const tol, ptiKruskalTensor * ktensor);
+int ptiCpdAlsHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank, ptiIndex const niters,
+                   double const tol, ptiRankKruskalTensor * ktensor);
+int ptiOmpCpdAlsHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank,
+                      ptiIndex const niters, double const tol, const int tk, const int tb,
+                      int balanced, ptiRankKruskalTensor * ktensor);
+
+/* ---------------------------------------------------------------------------
+ * Extensions (no reference counterpart): device-resident tensors.
+ * ------------------------------------------------------------------------ */
+typedef struct ptiB200Tensor ptiB200Tensor;
+
+/* Factor element types for the device entry points. */
+enum { PTI_B200_F32 = 0, PTI_B200_BF16 = 1 };
+
+/* Copy a COO or HiCOO tensor into device memory once.  The handle keeps the
+ * tensor, plus the per-mode schedules built on first use, until freed. */
+int ptiB200UploadSparseTensor(ptiB200Tensor **out, ptiSparseTensor const *X);
+int ptiB200UploadSparseTensorHiCOO(ptiB200Tensor **out, ptiSparseTensorHiCOO const *H);
+/* Build a device COO tensor from device arrays (inds[m] uint32 and vals f32,
+ * nnz entries each); the arrays are copied.  `stream` is a cudaStream_t. */
+int ptiB200TensorFromDeviceCOO(ptiB200Tensor **out, ptiIndex nmodes, const ptiIndex *ndims,
+                               ptiNnzIndex nnz, const ptiIndex * const *dev_inds,
+                               const ptiValue *dev_vals, void *stream);
+/* Convert a device COO handle to a device HiCOO handle on the GPU (same
+ * ordering rules as ptiSparseTensorToHiCOO); nb and max_nnzb may be NULL. */
+int ptiB200ConvertToHiCOO(ptiB200Tensor **out, ptiB200Tensor *coo, ptiElementIndex sb_bits,
+                          ptiElementIndex sk_bits, ptiElementIndex sc_bits,
+                          ptiNnzIndex *nb, ptiNnzIndex *max_nnzb, void *stream);
+/* Build the per-mode schedule for `mode` now (otherwise built on first use). */
+int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream);
+int ptiB200FreeTensor(ptiB200Tensor *t);
+/* Shape and statistics of a device tensor.  info: [nmodes, nnz, nb, sb, sk, sc, is_hicoo]. */
+int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndims_out);
+
+/* MTTKRP with everything in device memory.  dev_mats[k] points to ndims[k] x
+ * stride row-major factors of element type `factor_type`; dev_out receives
+ * ndims[mode] x stride FP32 rows (pad columns zeroed).  Runs asynchronously on
+ * `stream` (a cudaStream_t; NULL = legacy default stream). */
+int ptiB200MTTKRP(ptiB200Tensor *t, const void * const *dev_mats, int factor_type, ptiIndex rank,
+                  ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode, float *dev_out,
+                  void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPARTI_B200_H */
