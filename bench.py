@@ -1,0 +1,426 @@
+"""Benchmark: sparse HiCOO MTTKRP throughput on B200 (and CPD-ALS s/iter).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mttkrp|cpd]
+
+Default workload (mttkrp): 3rd-order tensor 200,000 x 150,000 x 20,000 with
+50M unique nonzeros, each mode's index Zipf(s=1.1) over a seeded permutation,
+values U(0,1) FP32; HiCOO sb=7 (sk=10, sc=14); FP32 factors U(0,1), R=32.
+One step = MTTKRP of all 3 modes.  The metric is algorithmic GB/s:
+    B(mode) = nnz*(N + 4) + nb*(8 + 4N) + 4*R*sum_m I_m
+(indices 1 B/mode + value, bptr + block indices, N-1 factor reads + 1 output).
+
+The timed tensor (0.8 GB) is larger than the 126 MB L2, so steps are not
+served from L2.  With --gpus N (torchrun) every rank runs its own replica of
+the workload (the path does not shard; no collective), value = all ranks'
+bytes / max time.
+
+--impl reference times the reference's own OpenMP CPU code (oracle/_ref,
+compiled from the reference sources) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+C2_DIMS = (200_000, 150_000, 20_000)
+C2_NNZ = 50_000_000
+C2_R = 32
+C2_SB, C2_SK, C2_SC = 7, 10, 14
+C3_DIMS = (20_000, 20_000, 20_000, 500)
+C3_NNZ = 40_000_000
+C3_R = 32
+C3_ITERS = 50
+SEED = 2024
+
+
+def hicoo_bytes(nnz, nb, dims, R, N, fsize=4):
+    return nnz * (N + 4) + nb * (8 + 4 * N) + fsize * R * sum(dims)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name>."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi every 200 ms while active."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_c2(device, seed):
+    """C2 tensor on the device: torch COO -> device HiCOO (GPU conversion)."""
+    import torch
+    from hiparti_b200 import DeviceTensor
+    from hiparti_b200.synth import coords_torch
+    inds = coords_torch(C2_DIMS, C2_NNZ, seed, zipf_s=1.1, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 1)
+    vals = torch.rand(C2_NNZ, generator=g, device=device, dtype=torch.float32)
+    coo = DeviceTensor.from_torch_coo(C2_DIMS, inds, vals)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h = coo.to_hicoo(C2_SB, C2_SK, C2_SC)
+    torch.cuda.synchronize()
+    conv_s = time.perf_counter() - t0
+    return coo, h, inds, vals, conv_s
+
+
+def c2_factors(device, seed):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 2)
+    stride = ((C2_R - 1) // 8 + 1) * 8
+    return [torch.rand((d, stride), generator=g, device=device, dtype=torch.float32) for d in C2_DIMS]
+
+
+def run_ours_mttkrp(args, rank, world):
+    import torch
+    from hiparti_b200 import HiCOOTensor, ffi, lib
+    dev = torch.device("cuda", torch.cuda.current_device())
+    coo, h, inds, vals, conv_s = make_c2(dev, SEED + rank)
+    nb = h.nb
+    mats = c2_factors(dev, SEED + rank)
+    stride = mats[0].shape[1]
+    N = 3
+    outs = [torch.empty((d, stride), dtype=torch.float32, device=dev) for d in C2_DIMS]
+    bytes_mode = [hicoo_bytes(C2_NNZ, nb, C2_DIMS, C2_R, N) for _ in range(N)]
+    step_bytes = sum(bytes_mode)
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        for m in range(N):
+            if ev is not None:
+                ev[m][0].record(stream)
+            h.mttkrp(mats, m, rank=C2_R, out=outs[m])
+            if ev is not None:
+                ev[m][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(N)] for _ in range(args.steps)]
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(ev[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    ms_total = max_over_ranks(ms_total, world)
+    ms_step = ms_total / args.steps
+    per_mode_ms = [statistics.mean(ev[k][m][0].elapsed_time(ev[k][m][1]) for k in range(args.steps))
+                   for m in range(N)]
+    value = step_bytes * world * args.steps / (ms_total * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    mean_launch_ms = statistics.mean(per_mode_ms)
+    achieved = statistics.mean(bytes_mode[m] / (per_mode_ms[m] * 1e-3) / 1e9 for m in range(N))
+    traffic = profile_traffic("hicoo_mttkrp_c2.txt")
+
+    # ---- end to end through the reference-facing C ABI (host buffers) ----
+    e2e = None
+    if rank == 0 or world > 1:
+        e2e = run_e2e(h, inds, vals, mats, nb, args)
+
+    result = {
+        "metric": "hicoo_mttkrp_GBps", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Zipf(1.1) coordinates, U(0,1) values and factors)",
+        "config": {"workload": "C2 HiCOO MTTKRP, 3-D 200000x150000x20000, 50M nnz Zipf(1.1), R=32, "
+                               "sb=7 sk=10 sc=14, FP32, all 3 modes per step",
+                   "nnz": C2_NNZ, "nb": nb, "rank": C2_R, "modes_per_step": N,
+                   "algorithmic_bytes_per_step": step_bytes,
+                   "l2": "inputs larger than L2 (tensor 0.8 GB vs 126 MB L2)",
+                   "parallelism": f"replicas x{world}", "conversion_s": round(conv_s, 3),
+                   "per_mode_ms": [round(x, 4) for x in per_mode_ms]},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "hicoo_tile_kernel (per-mode launch)",
+                     "mean_launch_ms": round(mean_launch_ms, 4)},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": N * args.steps,
+    }
+    return result
+
+
+def pinned_numpy(arr):
+    import torch
+    t = torch.empty(arr.shape, dtype=getattr(torch, str(arr.dtype)) if arr.dtype != np.uint32 else torch.int32,
+                    pin_memory=True)
+    out = t.numpy().view(arr.dtype)
+    out[...] = arr
+    return out, t
+
+
+def run_e2e(h_dev, inds, vals, mats, nb, args):
+    """The drop-in call ptiMTTKRPHiCOO with host (pinned) buffers: every call
+    copies the HiCOO tensor and factors to the device and the result back."""
+    import torch
+    from hiparti_b200 import COOTensor, HiCOOTensor
+    from hiparti_b200.api import _MatrixSet
+    from hiparti_b200._ffi import ffi, lib, check
+    # HiCOO arrays on the host: bring the device conversion's result back
+    host = download_hicoo(h_dev)
+    keep = []
+    def pin(a):
+        p, t = pinned_numpy(a)
+        keep.append(t)
+        return p
+    hh = HiCOOTensor(C2_DIMS, C2_SB, C2_SK, C2_SC, pin(host["bptr"]), [pin(b) for b in host["binds"]],
+                     [pin(e) for e in host["einds"]], pin(host["vals"]))
+    hmats = [pin(m.cpu().numpy()) for m in mats]
+    stride = hmats[0].shape[1]
+    out = pin(np.zeros((max(C2_DIMS), stride), np.float32))
+    ms = _MatrixSet(hmats + [out], C2_R)
+    N = 3
+    orders = [ffi.new("ptiIndex[]", [(m + i) % N for i in range(N)]) for m in range(N)]
+    L = lib()
+
+    def step():
+        for m in range(N):
+            check(L.ptiMTTKRPHiCOO(hh.c, ms.ptrs, orders[m], m), "ptiMTTKRPHiCOO")
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    ksteps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(ksteps):
+        step()
+    dt = (time.perf_counter() - t0) / ksteps
+    tensor_bytes = host["bptr"].nbytes + sum(b.nbytes for b in host["binds"]) + \
+        sum(e.nbytes for e in host["einds"]) + host["vals"].nbytes
+    fac_bytes = [m.nbytes for m in hmats]
+    h2d = sum(tensor_bytes + sum(fac_bytes) - fac_bytes[m] for m in range(N))
+    d2h = sum(C2_DIMS[m] * stride * 4 for m in range(N))
+    step_bytes = N * hicoo_bytes(C2_NNZ, nb, C2_DIMS, C2_R, N)
+    return {"value": round(step_bytes / dt / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": round(dt * 1e3, 3), "steps": ksteps,
+            "api": "ptiMTTKRPHiCOO (C ABI, host pinned buffers, tensor + factors copied in per call)"}
+
+
+def download_hicoo(h):
+    """Host copies of a device HiCOO tensor's arrays (bptr, binds, einds, vals)."""
+    from hiparti_b200._ffi import ffi, lib, check
+    info = h.info()
+    N, nnz, nb = info["nmodes"], info["nnz"], info["nb"]
+    bptr = np.empty(nb + 1, np.uint64)
+    binds = [np.empty(nb, np.uint32) for _ in range(N)]
+    einds = [np.empty(nnz, np.uint8) for _ in range(N)]
+    vals = np.empty(nnz, np.float32)
+    bp = ffi.new("ptiNnzIndex **")
+    args = ffi.new("void *[]", [ffi.cast("void *", binds[m].ctypes.data) for m in range(N)])
+    eargs = ffi.new("void *[]", [ffi.cast("void *", einds[m].ctypes.data) for m in range(N)])
+    check(lib().ptiB200DownloadHiCOO(h._h, ffi.cast("ptiNnzIndex *", bptr.ctypes.data), args, eargs,
+                                     ffi.cast("ptiValue *", vals.ctypes.data)), "ptiB200DownloadHiCOO")
+    return {"bptr": bptr, "binds": binds, "einds": einds, "vals": vals}
+
+
+def run_reference_arm(args, rank, world):
+    """Times the reference's own CPU code (oracle/_ref/libHiParTI.so, built
+    from its sources): ptiSparseTensorToHiCOO (tk=1, untimed) on a sample of
+    the C2 tensor, then ptiOmpMTTKRPHiCOO with every host thread, 3 modes per
+    step."""
+    if rank != 0:
+        return None
+    from oracle.oracle import Ref, ensure_built
+    from hiparti_b200.synth import coords_numpy
+    try:
+        ensure_built(ref=True)
+    except Exception:
+        pass
+    if not Ref.available():
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref not built (needs its sources)"}
+    ref = Ref()
+    threads = os.cpu_count() or 1
+    sample = args.ref_sample
+    inds = coords_numpy(C2_DIMS, sample, SEED, zipf_s=1.1)
+    vals = np.random.default_rng(SEED + 1).random(sample, dtype=np.float32)
+    h = ref.to_hicoo(list(C2_DIMS), inds, vals, C2_SB, C2_SK, C2_SC)
+    nb = h["bptr"].size - 1
+    rng = np.random.default_rng(SEED + 2)
+    stride = ((C2_R - 1) // 8 + 1) * 8
+    mats = [rng.random((d, stride), dtype=np.float32) for d in C2_DIMS]
+    N = 3
+    for _ in range(args.warmup):
+        for m in range(N):
+            ref.mttkrp_hicoo(list(C2_DIMS), h, mats, C2_R, m, variant="omp", tk=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for m in range(N):
+            ref.mttkrp_hicoo(list(C2_DIMS), h, mats, C2_R, m, variant="omp", tk=threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    step_bytes = N * hicoo_bytes(sample, nb, C2_DIMS, C2_R, N)
+    value = step_bytes / dt / 1e9
+    sample_desc = (f"{sample} unique nonzeros drawn by the C2 construction (same dims, Zipf(1.1) per mode, "
+                   f"U(0,1) values), nb={nb}; HiCOO built by the reference's ptiSparseTensorToHiCOO(tk=1), "
+                   f"untimed; one step = ptiOmpMTTKRPHiCOO(tk={threads}, tb=1) for modes 0,1,2")
+    return {"metric": "hicoo_mttkrp_GBps", "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "C2 HiCOO MTTKRP sample (reference ptiOmpMTTKRPHiCOO, tk=all host threads)",
+                       "nnz": sample, "nb": nb, "rank": C2_R},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+                             "sample": sample_desc},
+            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline_block(args):
+    """Reference OpenMP HiCOO MTTKRP on a bounded sample (rank 0, N=1)."""
+    res = run_reference_arm(argparse.Namespace(warmup=0, steps=1, ref_sample=args.ref_sample), 0, 1)
+    if res is None or "unavailable" in res:
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": res.get("unavailable") if res else "n/a"}
+    return res["cpu_baseline"]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mttkrp", choices=["mttkrp"])
+    ap.add_argument("--ref-sample", type=int, default=4_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        res = run_reference_arm(args, rank, world)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+        return
+
+    from hiparti_b200 import build
+    build.build()
+    rank, world, _ = dist_setup(args.gpus)
+    res = run_ours_mttkrp(args, rank, world)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline_block(args)
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

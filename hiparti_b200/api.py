@@ -1,0 +1,361 @@
+"""Python mirror of the reference's Python layer (HiParTIPy/Tensor.py,
+HiParTIPy/Matrix.py) for the MTTKRP / CPD path, over the C ABI.
+
+Host-side objects (``COOTensor``, ``HiCOOTensor``) hold numpy arrays and hand
+the library struct views of them, so every call goes through the same C entry
+points a C program uses.  ``DeviceTensor`` keeps a tensor resident on the GPU
+(``ptiB200*`` extensions) and takes torch CUDA tensors as factors.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ._ffi import PtiError, check, ffi, lib
+
+_F32 = 0
+_BF16 = 1
+
+
+def _stride(R: int) -> int:
+    return ((R - 1) // 8 + 1) * 8
+
+
+def _ptr(arr, ctype):
+    return ffi.cast(ctype, arr.ctypes.data)
+
+
+class _MatrixSet:
+    """N+1 ptiMatrix structs over numpy arrays (factors + output)."""
+
+    def __init__(self, arrays, R):
+        self.arrays = arrays
+        self.structs = ffi.new("ptiMatrix[]", len(arrays))
+        self.ptrs = ffi.new("ptiMatrix *[]", len(arrays))
+        for i, a in enumerate(arrays):
+            s = self.structs[i]
+            s.nrows = a.shape[0]
+            s.ncols = R
+            s.cap = a.shape[0]
+            s.stride = a.shape[1]
+            s.values = _ptr(a, "float *")
+            self.ptrs[i] = ffi.addressof(self.structs, i)
+
+
+class COOTensor:
+    """A COO sparse tensor whose index/value arrays live in numpy."""
+
+    def __init__(self, dims, inds, vals):
+        self.dims = [int(d) for d in dims]
+        self.inds = [np.ascontiguousarray(i, dtype=np.uint32) for i in inds]
+        self.vals = np.ascontiguousarray(vals, dtype=np.float32)
+        if len(self.inds) != len(self.dims):
+            raise ValueError("one index array per mode")
+        if any(i.size != self.vals.size for i in self.inds):
+            raise ValueError("index and value arrays differ in length")
+        self._build()
+
+    @classmethod
+    def load(cls, fname: str, start_index: int = 1) -> "COOTensor":
+        """ptiLoadSparseTensor (text .tns or SPLATT .bin)."""
+        t = ffi.new("ptiSparseTensor *")
+        check(lib().ptiLoadSparseTensor(t, start_index, fname.encode()), "ptiLoadSparseTensor")
+        N, nnz = t.nmodes, t.nnz
+        dims = [t.ndims[m] for m in range(N)]
+        inds = [np.frombuffer(ffi.buffer(t.inds[m].data, 4 * nnz), np.uint32).copy() for m in range(N)]
+        vals = np.frombuffer(ffi.buffer(t.values.data, 4 * nnz), np.float32).copy()
+        lib().ptiFreeSparseTensor(t)
+        return cls(dims, inds, vals)
+
+    def _build(self):
+        N = len(self.dims)
+        self._dims = np.asarray(self.dims, np.uint32)
+        self._so = np.arange(N, dtype=np.uint32)
+        self._vecs = ffi.new("ptiIndexVector[]", N)
+        for m in range(N):
+            self._vecs[m].len = self._vecs[m].cap = self.vals.size
+            self._vecs[m].data = _ptr(self.inds[m], "ptiIndex *")
+        self.c = ffi.new("ptiSparseTensor *")
+        self.c.nmodes = N
+        self.c.sortorder = _ptr(self._so, "ptiIndex *")
+        self.c.ndims = _ptr(self._dims, "ptiIndex *")
+        self.c.nnz = self.vals.size
+        self.c.inds = self._vecs
+        self.c.values.len = self.c.values.cap = self.vals.size
+        self.c.values.data = _ptr(self.vals, "ptiValue *")
+
+    @property
+    def nmodes(self):
+        return len(self.dims)
+
+    @property
+    def nnz(self):
+        return int(self.vals.size)
+
+    def mttkrp(self, mats, R, mode, variant="seq"):
+        """Runs the reference entry point `variant` ("seq" -> ptiMTTKRP, "omp"
+        -> ptiOmpMTTKRP, "cuda" -> ptiCudaMTTKRP, "onekernel" ->
+        ptiCudaMTTKRPOneKernel) on the GPU; returns (dims[mode], stride)."""
+        return _host_mttkrp(self, mats, R, mode, variant)
+
+    def to_hicoo(self, sb=7, sk=10, sc=14) -> "HiCOOTensor":
+        """ptiSparseTensorToHiCOO (GPU).  As in the reference, this tensor's
+        arrays are left sorted in HiCOO order."""
+        h = ffi.new("ptiSparseTensorHiCOO *")
+        maxnb = ffi.new("ptiNnzIndex *")
+        check(lib().ptiSparseTensorToHiCOO(h, maxnb, self.c, sb, sk, sc, 1), "ptiSparseTensorToHiCOO")
+        out = HiCOOTensor._from_struct(h, int(maxnb[0]))
+        lib().ptiFreeSparseTensorHiCOO(h)
+        return out
+
+    def cpd_als(self, R, niters, tol=0.0, variant="seq"):
+        return _host_cpd(self, R, niters, tol, variant)
+
+
+class HiCOOTensor:
+    """A HiCOO tensor held as numpy arrays (the fields of ptiSparseTensorHiCOO)."""
+
+    def __init__(self, dims, sb, sk, sc, bptr, binds, einds, vals, kptr=None, cptr=None,
+                 knnzs=None, nkiters=None, kschr_rows=None, max_nnzb=0, balanced=None):
+        self.dims = [int(d) for d in dims]
+        self.sb, self.sk, self.sc = int(sb), int(sk), int(sc)
+        self.bptr = np.ascontiguousarray(bptr, np.uint64)
+        self.binds = [np.ascontiguousarray(b, np.uint32) for b in binds]
+        self.einds = [np.ascontiguousarray(e, np.uint8) for e in einds]
+        self.vals = np.ascontiguousarray(vals, np.float32)
+        self.kptr = None if kptr is None else np.ascontiguousarray(kptr, np.uint64)
+        self.cptr = None if cptr is None else np.ascontiguousarray(cptr, np.uint64)
+        self.knnzs = None if knnzs is None else np.ascontiguousarray(knnzs, np.uint64)
+        self.nkiters = None if nkiters is None else np.ascontiguousarray(nkiters, np.uint32)
+        self.kschr_rows = kschr_rows
+        self.max_nnzb = max_nnzb
+        self.balanced = balanced  # dict: rows, pos_rows, rest, nkpars (from the converter)
+        self._build()
+
+    @classmethod
+    def _from_struct(cls, h, max_nnzb):
+        N, nnz = h.nmodes, h.nnz
+        nb = h.bptr.len - 1
+
+        def arr(vec, n, dt):
+            return np.frombuffer(ffi.buffer(vec.data, n * np.dtype(dt).itemsize), dt).copy() if n else np.empty(0, dt)
+        dims = [h.ndims[m] for m in range(N)]
+        rows, brows, prows, rest = [], [], [], []
+        for m in range(N):
+            for i in range((dims[m] + (1 << h.sk_bits) - 1) >> h.sk_bits):
+                rows.append(arr(h.kschr[m][i], h.kschr[m][i].len, np.uint32))
+                brows.append(arr(h.kschr_balanced[m][i], h.kschr_balanced[m][i].len, np.uint32))
+                prows.append(arr(h.kschr_balanced_pos[m][i], h.kschr_balanced_pos[m][i].len, np.uint32))
+            rest.append(arr(h.kschr_rest[m], h.kschr_rest[m].len, np.uint32))
+        balanced = {"rows": brows, "pos_rows": prows, "rest": rest,
+                    "nkpars": np.array([h.nkpars[m] for m in range(N)], np.uint32)}
+        return cls(dims, h.sb_bits, h.sk_bits, h.sc_bits,
+                   arr(h.bptr, nb + 1, np.uint64),
+                   [arr(h.binds[m], nb, np.uint32) for m in range(N)],
+                   [arr(h.einds[m], nnz, np.uint8) for m in range(N)],
+                   arr(h.values, nnz, np.float32),
+                   kptr=arr(h.kptr, h.kptr.len, np.uint64), cptr=arr(h.cptr, h.cptr.len, np.uint64),
+                   knnzs=arr(h.knnzs, h.knnzs.len, np.uint64),
+                   nkiters=np.array([h.nkiters[m] for m in range(N)], np.uint32),
+                   kschr_rows=rows, max_nnzb=max_nnzb, balanced=balanced)
+
+    def _build(self):
+        N = len(self.dims)
+        nb = self.bptr.size - 1
+        nnz = self.vals.size
+        self._dims = np.asarray(self.dims, np.uint32)
+        self._so = np.arange(N, dtype=np.uint32)
+        self._bv = ffi.new("ptiBlockIndexVector[]", N)
+        self._ev = ffi.new("ptiElementIndexVector[]", N)
+        for m in range(N):
+            self._bv[m].len = self._bv[m].cap = nb
+            self._bv[m].data = _ptr(self.binds[m], "ptiBlockIndex *")
+            self._ev[m].len = self._ev[m].cap = nnz
+            self._ev[m].data = _ptr(self.einds[m], "ptiElementIndex *")
+        c = ffi.new("ptiSparseTensorHiCOO *")
+        c.nmodes = N
+        c.sortorder = _ptr(self._so, "ptiIndex *")
+        c.ndims = _ptr(self._dims, "ptiIndex *")
+        c.nnz = nnz
+        c.sb_bits, c.sk_bits, c.sc_bits = self.sb, self.sk, self.sc
+        c.bptr.len = c.bptr.cap = nb + 1
+        c.bptr.data = _ptr(self.bptr, "ptiNnzIndex *")
+        c.binds = self._bv
+        c.einds = self._ev
+        c.values.len = c.values.cap = nnz
+        c.values.data = _ptr(self.vals, "ptiValue *")
+        if self.kptr is not None:
+            c.kptr.len = c.kptr.cap = self.kptr.size
+            c.kptr.data = _ptr(self.kptr, "ptiNnzIndex *")
+        self.c = c
+
+    @property
+    def nmodes(self):
+        return len(self.dims)
+
+    @property
+    def nnz(self):
+        return int(self.vals.size)
+
+    @property
+    def nb(self):
+        return int(self.bptr.size - 1)
+
+    def mttkrp(self, mats, R, mode, variant="seq"):
+        """"seq" -> ptiMTTKRPHiCOO, "omp" -> ptiOmpMTTKRPHiCOO, "cuda" ->
+        ptiCudaMTTKRPHiCOO; all on the GPU."""
+        return _host_mttkrp(self, mats, R, mode, variant)
+
+
+def _host_mttkrp(t, mats, R, mode, variant):
+    N = t.nmodes
+    mats = [np.ascontiguousarray(m, np.float32) for m in mats]
+    stride = mats[0].shape[1]
+    out = np.zeros((max(t.dims), stride), np.float32)
+    ms = _MatrixSet(mats + [out], R)
+    order = ffi.new("ptiIndex[]", [(mode + i) % N for i in range(N)])
+    L = lib()
+    if isinstance(t, COOTensor):
+        fn = {"seq": lambda: L.ptiMTTKRP(t.c, ms.ptrs, order, mode),
+              "omp": lambda: L.ptiOmpMTTKRP(t.c, ms.ptrs, order, mode, 8),
+              "cuda": lambda: L.ptiCudaMTTKRP(t.c, ms.ptrs, order, mode, 5),
+              "onekernel": lambda: L.ptiCudaMTTKRPOneKernel(t.c, ms.ptrs, order, mode, 15)}[variant]
+    else:
+        fn = {"seq": lambda: L.ptiMTTKRPHiCOO(t.c, ms.ptrs, order, mode),
+              "omp": lambda: L.ptiOmpMTTKRPHiCOO(t.c, ms.ptrs, order, mode, 8, 1),
+              "cuda": lambda: L.ptiCudaMTTKRPHiCOO(t.c, ms.ptrs, order, mode, 0, 1)}[variant]
+    check(fn(), f"MTTKRP[{variant}]")
+    return out[: t.dims[mode]].copy()
+
+
+def _host_cpd(t, R, niters, tol, variant):
+    L = lib()
+    k = ffi.new("ptiKruskalTensor *")
+    dims = ffi.new("ptiIndex[]", t.dims)
+    check(L.ptiNewKruskalTensor(k, t.nmodes, dims, R), "ptiNewKruskalTensor")
+    fn = {"seq": lambda: L.ptiCpdAls(t.c, R, niters, tol, k),
+          "omp": lambda: L.ptiOmpCpdAls(t.c, R, niters, tol, 8, 0, k),
+          "cuda": lambda: L.ptiCudaCpdAls(t.c, R, niters, tol, k)}[variant]
+    try:
+        check(fn(), f"CpdAls[{variant}]")
+        lam = np.frombuffer(ffi.buffer(getattr(k, "lambda"), 4 * R), np.float32).copy()
+        facs = []
+        for m in range(t.nmodes):
+            f = k.factors[m]
+            a = np.frombuffer(ffi.buffer(f.values, 4 * f.nrows * f.stride), np.float32)
+            facs.append(a.reshape(f.nrows, f.stride)[:, :R].copy())
+        return dict(fit=k.fit, lambda_=lam, factors=facs)
+    finally:
+        L.ptiFreeKruskalTensor(k)
+
+
+# ----------------------------------------------------------------------------
+# Device-resident tensors (torch)
+# ----------------------------------------------------------------------------
+class DeviceTensor:
+    """A tensor kept in GPU memory through the ptiB200 extension entry points."""
+
+    def __init__(self, handle, dims):
+        self._h = handle
+        self.dims = list(dims)
+
+    @classmethod
+    def from_coo(cls, t: COOTensor) -> "DeviceTensor":
+        hp = ffi.new("ptiB200Tensor **")
+        check(lib().ptiB200UploadSparseTensor(hp, t.c), "ptiB200UploadSparseTensor")
+        return cls(hp[0], t.dims)
+
+    @classmethod
+    def from_hicoo(cls, t: HiCOOTensor) -> "DeviceTensor":
+        hp = ffi.new("ptiB200Tensor **")
+        check(lib().ptiB200UploadSparseTensorHiCOO(hp, t.c), "ptiB200UploadSparseTensorHiCOO")
+        return cls(hp[0], t.dims)
+
+    @classmethod
+    def from_torch_coo(cls, dims, inds, vals) -> "DeviceTensor":
+        """inds: list of int32/uint32-valued CUDA tensors (nnz,), vals: float32 (nnz,)."""
+        import torch
+        N = len(dims)
+        inds = [i.contiguous() for i in inds]
+        vals = vals.contiguous().to(torch.float32)
+        ip = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", i.data_ptr()) for i in inds])
+        d = ffi.new("ptiIndex[]", [int(x) for x in dims])
+        hp = ffi.new("ptiB200Tensor **")
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200TensorFromDeviceCOO(hp, N, d, vals.numel(), ip,
+                                               ffi.cast("ptiValue *", vals.data_ptr()), stream),
+              "ptiB200TensorFromDeviceCOO")
+        return cls(hp[0], dims)
+
+    def to_hicoo(self, sb=7, sk=10, sc=14) -> "DeviceTensor":
+        import torch
+        hp = ffi.new("ptiB200Tensor **")
+        nb = ffi.new("ptiNnzIndex *")
+        mx = ffi.new("ptiNnzIndex *")
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200ConvertToHiCOO(hp, self._h, sb, sk, sc, nb, mx, stream), "ptiB200ConvertToHiCOO")
+        out = DeviceTensor(hp[0], self.dims)
+        out.nb, out.max_nnzb = int(nb[0]), int(mx[0])
+        return out
+
+    def info(self):
+        info = ffi.new("ptiNnzIndex[7]")
+        check(lib().ptiB200TensorInfo(self._h, info, ffi.NULL), "ptiB200TensorInfo")
+        keys = ["nmodes", "nnz", "nb", "sb", "sk", "sc", "hicoo"]
+        return {k: int(info[i]) for i, k in enumerate(keys)}
+
+    def prepare(self, mode=None):
+        import torch
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        modes = range(len(self.dims)) if mode is None else [mode]
+        for m in modes:
+            check(lib().ptiB200Prepare(self._h, m, stream), "ptiB200Prepare")
+
+    def mttkrp(self, factors, mode, rank=None, out=None, mats_order=None):
+        """factors: list of CUDA tensors (I_k, stride), float32 or bfloat16, all
+        of one dtype; returns / fills a float32 (I_mode, stride) tensor."""
+        import torch
+        N = len(self.dims)
+        ft = factors[0].dtype
+        if ft not in (torch.float32, torch.bfloat16) or any(f.dtype != ft for f in factors):
+            raise TypeError("factors must all be float32 or all bfloat16")
+        stride = factors[0].shape[1]
+        R = stride if rank is None else int(rank)
+        if out is None:
+            out = torch.empty((self.dims[mode], stride), dtype=torch.float32, device=factors[0].device)
+        if mats_order is None:
+            mats_order = [(mode + i) % N for i in range(N)]
+        mp = ffi.new("void *[]", [ffi.cast("void *", f.data_ptr()) for f in factors])
+        order = ffi.new("ptiIndex[]", list(mats_order))
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200MTTKRP(self._h, mp, _F32 if ft == torch.float32 else _BF16, R, stride, order,
+                                  mode, ffi.cast("float *", out.data_ptr()), stream), "ptiB200MTTKRP")
+        return out
+
+    def cpd_als(self, factors, niters, tol=0.0, precision="fp32", fp32_sweeps=1, rank=None):
+        """CPD-ALS on the device (ptiB200CpdAls).  factors: list of float32 CUDA
+        tensors (I_k, stride) holding the initial factors; updated in place.
+        precision "bf16" makes the MTTKRP gathers read BF16 copies for all but
+        the last fp32_sweeps iterations.  Returns (lambda, fits)."""
+        import torch
+        stride = factors[0].shape[1]
+        R = stride if rank is None else int(rank)
+        lam = torch.empty(R, dtype=torch.float32, device=factors[0].device)
+        fits = ffi.new("double[]", max(int(niters), 1))
+        done = ffi.new("ptiIndex *")
+        fp = ffi.new("float *[]", [ffi.cast("float *", f.data_ptr()) for f in factors])
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        prec = {"fp32": _F32, "bf16": _BF16}[precision]
+        check(lib().ptiB200CpdAls(self._h, R, niters, tol, prec, fp32_sweeps, fp, stride,
+                                  ffi.cast("float *", lam.data_ptr()), fits, done, stream), "ptiB200CpdAls")
+        return lam, [fits[i] for i in range(done[0])]
+
+    def free(self):
+        if self._h is not None:
+            lib().ptiB200FreeTensor(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -86,6 +86,10 @@ struct DevBuf {
 // unlimited) so that stream-ordered allocations are served from the pool.
 void configure_pool_once();
 
+// Allocation sizes are rounded up to 64 bytes plus one 64-byte guard so that
+// vectorised and bulk copies of a final partial tile stay inside the buffer.
+inline size_t padded(size_t bytes) { return ((bytes + 63) / 64) * 64 + 64; }
+
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int sm_count();

@@ -1,0 +1,617 @@
+// cpd.cu -- CPD-ALS on the GPU, restating the loop of src/sptensor/cpd.c:32-160:
+//
+//   for it: for m:  M   = MTTKRP(X, A, m)
+//                   A_m = M * (Hadamard_{k != m} A_k^T A_k)^{-1}
+//                   lambda = it == 0 ? column 2-norms : max(column max, 1);  A_m /= lambda
+//                   G_m = A_m^T A_m
+//           fit = 1 - sqrt(||X||^2 + lambda^T (Hadamard_k G_k) lambda - 2 <X, M_{N-1} o A_{N-1} lambda>) / ||X||
+//   final lambda: lambda_r *= prod_m ||A_m[:, r]||, columns normalised
+//
+// Precision: factors are stored in FP32 (or, in mixed mode, additionally as a
+// BF16 copy that the MTTKRP gathers read); MTTKRP accumulates in FP32; Grams,
+// their Hadamard product, the Cholesky factor and inverse, the row solve and
+// the fit are FP64.  A Gram matrix that is not positive definite is inverted
+// by Gauss-Jordan elimination with partial pivoting (the reference falls back
+// to sgesv, src/matrix/matrix_solver.c:66-80); a singular one leaves the rows
+// unsolved, as sgesv does when it fails.
+//
+// The fit uses the full symmetric Grams.  (The reference's KruskalTensorFit,
+// src/ktensor/ktensor.c:105-147, reads the triangle of each Gram that its
+// ssyrk_ call does not write, so its printed fit is not the model's fit.)
+#include <cuda_bf16.h>
+
+#include "tensor.cuh"
+
+namespace pti {
+
+constexpr int kMaxCpdRank = 128;
+
+// Gram accumulation: G += A^T A over rows [0, I).  If inv_scale is given the
+// rows are first divided column-wise by lambda (and written back); if bf16 is
+// given the (scaled) rows are also stored as BF16.  Dynamic shared memory:
+// R*R doubles of accumulator + 32*R doubles of row tile.
+__global__ void gram_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, const float *lambda,
+                            __nv_bfloat16 *bf16, double *G)
+{
+    extern __shared__ double sm[];
+    double *acc = sm;
+    double *tile = sm + (size_t)R * R;
+    const uint32_t RR = R * R;
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) acc[e] = 0.0;
+    for (uint64_t r0 = (uint64_t)blockIdx.x * 32; r0 < I; r0 += (uint64_t)gridDim.x * 32) {
+        const uint32_t rows = (uint32_t)((I - r0) < 32 ? (I - r0) : 32);
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < 32 * stride; e += blockDim.x) {
+            const uint32_t r = e / stride, c = e % stride;
+            if (r >= rows) continue;
+            float *p = A + (r0 + r) * stride + c;
+            float v = *p;
+            if (c >= R) {
+                v = 0.f;
+                if (lambda) *p = 0.f;
+            } else if (lambda) {
+                v = v / lambda[c];
+                *p = v;
+            }
+            if (bf16) bf16[(r0 + r) * stride + c] = __float2bfloat16_rn(v);
+            if (c < R) tile[r * R + c] = (double)v;
+        }
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+            const uint32_t p = e / R, q = e % R;
+            double s = 0.0;
+            for (uint32_t r = 0; r < rows; ++r) s += tile[r * R + p] * tile[r * R + q];
+            acc[e] += s;
+        }
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) atomicAdd(G + e, acc[e]);
+}
+
+// One CTA: W = (Hadamard_{k != mode} G_k)^{-1}.  work holds 3*R*R doubles.
+// flag[0] = 1 if the Cholesky factorisation failed (fallback used), 2 if the
+// matrix was singular (W = identity: rows left unsolved).
+__global__ void gram_inverse_kernel(const double *G, uint32_t N, uint32_t R, uint32_t mode, double *W,
+                                    double *work, int *flag)
+{
+    const uint32_t RR = R * R;
+    double *V = work, *L = work + RR, *Li = work + 2 * RR;
+    __shared__ int s_bad;
+    __shared__ double s_d;
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+        double v = 1.0;
+        for (uint32_t k = 1; k < N; ++k) v *= G[(size_t)((mode + k) % N) * RR + e];
+        V[e] = v;
+        L[e] = 0.0;
+        Li[e] = 0.0;
+    }
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    // Cholesky V = L L^T, column by column
+    for (uint32_t j = 0; j < R; ++j) {
+        if (threadIdx.x == 0) {
+            double d = V[j * R + j];
+            for (uint32_t k = 0; k < j; ++k) d -= L[j * R + k] * L[j * R + k];
+            if (!(d > 0.0)) s_bad = 1;
+            s_d = d > 0.0 ? sqrt(d) : 1.0;
+            L[j * R + j] = s_d;
+        }
+        __syncthreads();
+        if (s_bad) break;
+        for (uint32_t i = j + 1 + threadIdx.x; i < R; i += blockDim.x) {
+            double s = V[i * R + j];
+            for (uint32_t k = 0; k < j; ++k) s -= L[i * R + k] * L[j * R + k];
+            L[i * R + j] = s / s_d;
+        }
+        __syncthreads();
+    }
+    if (!s_bad) {
+        // Li = L^{-1}, one column per thread
+        for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+            for (uint32_t i = c; i < R; ++i) {
+                double s = (i == c) ? 1.0 : 0.0;
+                for (uint32_t k = c; k < i; ++k) s -= L[i * R + k] * Li[k * R + c];
+                Li[i * R + c] = s / L[i * R + i];
+            }
+        }
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+            const uint32_t p = e / R, q = e % R;
+            double s = 0.0;
+            for (uint32_t k = max(p, q); k < R; ++k) s += Li[k * R + p] * Li[k * R + q];
+            W[e] = s;
+        }
+        if (threadIdx.x == 0) flag[0] = 0;
+        return;
+    }
+    // Gauss-Jordan with partial pivoting on [V | I]: L holds V, Li holds I.
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+        L[e] = V[e];
+        Li[e] = (e / R == e % R) ? 1.0 : 0.0;
+    }
+    __shared__ uint32_t s_piv;
+    __shared__ int s_sing;
+    if (threadIdx.x == 0) s_sing = 0;
+    __syncthreads();
+    for (uint32_t j = 0; j < R && !s_sing; ++j) {
+        if (threadIdx.x == 0) {
+            uint32_t p = j;
+            for (uint32_t i = j + 1; i < R; ++i)
+                if (fabs(L[i * R + j]) > fabs(L[p * R + j])) p = i;
+            s_piv = p;
+            if (L[p * R + j] == 0.0) s_sing = 1;
+        }
+        __syncthreads();
+        if (s_sing) break;
+        const uint32_t p = s_piv;
+        if (p != j)
+            for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+                double t = L[j * R + c]; L[j * R + c] = L[p * R + c]; L[p * R + c] = t;
+                t = Li[j * R + c]; Li[j * R + c] = Li[p * R + c]; Li[p * R + c] = t;
+            }
+        __syncthreads();
+        const double piv = L[j * R + j];
+        __syncthreads();
+        for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+            L[j * R + c] /= piv;
+            Li[j * R + c] /= piv;
+        }
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+            const uint32_t i = e / R, c = e % R;
+            if (i == j) continue;
+            const double f = L[i * R + j];
+            if (c != j) L[i * R + c] -= f * L[j * R + c];
+            Li[i * R + c] -= f * Li[j * R + c];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x)
+            if (i != j) L[i * R + j] = 0.0;
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x)
+        W[e] = s_sing ? ((e / R == e % R) ? 1.0 : 0.0) : Li[e];
+    if (threadIdx.x == 0) flag[0] = s_sing ? 2 : 1;
+}
+
+// A[i, :] = M[i, :] * W (W symmetric), FP64 accumulation; pad columns zeroed.
+// Accumulates per-column sums of squares (FP64) and maxima of the FP32 results.
+__global__ void solve_rows_kernel(const float *M, const double *W, uint32_t I, uint32_t R, uint32_t stride, float *A,
+                                  double *colsq, int *colmax)
+{
+    extern __shared__ double sm[];
+    double *sW = sm;                         // R*R
+    double *s_sq = sm + (size_t)R * R;       // R
+    int *s_mx = reinterpret_cast<int *>(s_sq + R);  // R
+    for (uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) sW[e] = W[e];
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        s_sq[c] = 0.0;
+        s_mx[c] = 0;  // bits of +0.0f
+    }
+    __syncthreads();
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = e / stride;
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c >= R) {
+            A[e] = 0.f;
+            continue;
+        }
+        const float *m = M + i * stride;
+        double s = 0.0;
+        for (uint32_t k = 0; k < R; ++k) s += (double)m[k] * sW[k * R + c];
+        const float v = (float)s;
+        A[e] = v;
+        atomicAdd(&s_sq[c], (double)v * (double)v);
+        if (v > 0.f) atomicMax(&s_mx[c], __float_as_int(v));
+    }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        atomicAdd(&colsq[c], s_sq[c]);
+        atomicMax(&colmax[c], s_mx[c]);
+    }
+}
+
+// lambda from the column statistics: iteration 0 -> 2-norm
+// (src/matrix/matrix.c:389-469), later -> max(column max, 1) (:472-553).
+__global__ void lambda_kernel(const double *colsq, const int *colmax, uint32_t R, int use_2norm, float *lambda)
+{
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        if (use_2norm) {
+            lambda[c] = (float)sqrt(colsq[c]);
+        } else {
+            float v = __int_as_float(colmax[c]);
+            lambda[c] = v < 1.f ? 1.f : v;
+        }
+    }
+}
+
+// inner += sum_i sum_r lambda_r A[i, r] M[i, r]
+__global__ void inner_kernel(const float *A, const float *M, uint32_t I, uint32_t R, uint32_t stride,
+                             const float *lambda, double *inner)
+{
+    double s = 0.0;
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c < R) s += (double)A[e] * (double)M[e] * (double)lambda[c];
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(inner, s);
+}
+
+__global__ void sumsq_kernel(const float *v, uint64_t n, double *out)
+{
+    double s = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        s += (double)v[i] * (double)v[i];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// fit = 1 - sqrt(normX2 + |lambda^T (Hadamard_k G_k) lambda| - 2 inner) / sqrt(normX2)
+// (src/ktensor/ktensor.c:77-99: the square root is skipped if the residual is
+// not positive).
+__global__ void fit_kernel(const double *G, uint32_t N, uint32_t R, const float *lambda, const double *normX2,
+                           const double *inner, double *fit_out)
+{
+    __shared__ double s_part[32];
+    double s = 0.0;
+    for (uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+        double v = 1.0;
+        for (uint32_t k = 0; k < N; ++k) v *= G[(size_t)k * R * R + e];
+        s += v * (double)lambda[e / R] * (double)lambda[e % R];
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double norm_mats = 0.0;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) norm_mats += s_part[w];
+        norm_mats = fabs(norm_mats);
+        double residual = normX2[0] + norm_mats - 2.0 * inner[0];
+        if (residual > 0.0) residual = sqrt(residual);
+        fit_out[0] = 1.0 - residual / sqrt(normX2[0]);
+    }
+}
+
+// Column 2-norms of A (FP64), for the final lambda.
+__global__ void colsq_kernel(const float *A, uint32_t I, uint32_t R, uint32_t stride, double *colsq)
+{
+    extern __shared__ double s_sq[];
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) s_sq[c] = 0.0;
+    __syncthreads();
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c < R) atomicAdd(&s_sq[c], (double)A[e] * (double)A[e]);
+    }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) atomicAdd(&colsq[c], s_sq[c]);
+}
+
+// A[:, c] /= norm_c ; lambda_c *= norm_c (src/matrix/matrix.c:556-572)
+__global__ void final_scale_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, const double *colsq,
+                                   float *lambda, int update_lambda)
+{
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c < R) A[e] = A[e] / (float)sqrt(colsq[c]);
+    }
+    if (update_lambda && blockIdx.x == 0)
+        for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) lambda[c] *= (float)sqrt(colsq[c]);
+}
+
+int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
+                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// The ALS driver.
+// ---------------------------------------------------------------------------
+struct CpdOptions {
+    uint32_t R = 0, niters = 0;
+    double tol = 0.0;
+    int precision = PTI_B200_F32;  // factors read by MTTKRP: F32 or BF16
+    uint32_t fp32_sweeps = 1;      // closing iterations with FP32 factors (mixed mode)
+};
+
+struct CpdResult {
+    std::vector<double> fits;
+    uint32_t iters = 0;
+    int solver_flags = 0;  // OR of gram_inverse flags seen
+};
+
+// A[m] (device, I_m x stride FP32) hold the initial factors on entry and the
+// result on exit; lambda (device, R floats) receives the weights.
+int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda, const CpdOptions &opt,
+               CpdResult &res, cudaStream_t s)
+{
+    const char *mod = "B200 CPD-ALS";
+    const uint32_t N = t->nmodes, R = opt.R;
+    PTI_CHECK(R >= 1 && R <= (uint32_t)kMaxCpdRank, PTIERR_VALUE_ERROR, mod, "rank must be in [1, 128]");
+    PTI_CHECK(stride >= R && stride % 8 == 0, PTIERR_SHAPE_MISMATCH, mod, "stride must be >= rank, multiple of 8");
+    PTI_CHECK(opt.precision == PTI_B200_F32 || opt.precision == PTI_B200_BF16, PTIERR_VALUE_ERROR, mod,
+              "bad precision");
+    const uint32_t RR = R * R;
+    uint32_t maxI = 0;
+    for (uint32_t m = 0; m < N; ++m) maxI = std::max(maxI, t->ndims[m]);
+
+    DevBuf M, G, W, work, stats, scal, Ab[kMaxModes];
+    PTI_CUDA(M.alloc(padded((size_t)maxI * stride * 4), s), mod);
+    PTI_CUDA(G.alloc(padded((size_t)N * RR * 8), s), mod);
+    PTI_CUDA(W.alloc(padded((size_t)RR * 8), s), mod);
+    PTI_CUDA(work.alloc(padded((size_t)3 * RR * 8), s), mod);
+    PTI_CUDA(stats.alloc(padded((size_t)R * 12 + 64), s), mod);  // colsq (R doubles) + colmax (R ints)
+    // scal: [0] normX2, [1] inner, [2..2+niters) fits ; flags after
+    PTI_CUDA(scal.alloc(padded((size_t)(4 + opt.niters) * 8 + 64), s), mod);
+    double *colsq = stats.as<double>();
+    int *colmax = reinterpret_cast<int *>(colsq + R);
+    double *normX2 = scal.as<double>(), *inner = normX2 + 1, *fits = normX2 + 2;
+    int *flag = reinterpret_cast<int *>(fits + opt.niters + 1);
+    const bool mixed = opt.precision == PTI_B200_BF16;
+    if (mixed)
+        for (uint32_t m = 0; m < N; ++m)
+            PTI_CUDA(Ab[m].alloc(padded((size_t)t->ndims[m] * stride * 2), s), mod);
+
+    const size_t gram_smem = (size_t)(RR + 32 * R) * 8;
+    const size_t solve_smem = (size_t)RR * 8 + (size_t)R * 12;
+    PTI_CUDA(cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem), mod);
+    PTI_CUDA(cudaFuncSetAttribute(solve_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem), mod);
+    const unsigned sms = (unsigned)sm_count();
+    auto rows_grid = [&](uint64_t items, unsigned per) {
+        return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + per - 1) / per, sms * 4ull));
+    };
+
+    // initial Grams (cpd.c:65-72) and BF16 copies
+    PTI_CUDA(cudaMemsetAsync(G.ptr, 0, (size_t)N * RR * 8, s), mod);
+    for (uint32_t m = 0; m < N; ++m)
+        gram_kernel<<<rows_grid(t->ndims[m], 32), 256, gram_smem, s>>>(
+            A[m], t->ndims[m], R, stride, nullptr, mixed ? Ab[m].as<__nv_bfloat16>() : nullptr, G.as<double>() + (size_t)m * RR);
+    PTI_CUDA(cudaMemsetAsync(scal.ptr, 0, 16, s), mod);
+    if (t->nnz) sumsq_kernel<<<rows_grid(t->nnz, 256), 256, 0, s>>>(t->vals.as<float>(), t->nnz, normX2);
+    PTI_CUDA(cudaGetLastError(), mod);
+
+    std::vector<uint32_t> order(N);
+    std::vector<const void *> fptr(N);
+    res.fits.clear();
+    double oldfit = 0.0;
+    uint32_t it = 0;
+    for (; it < opt.niters; ++it) {
+        const bool use_bf16 = mixed && it + opt.fp32_sweeps < opt.niters;
+        for (uint32_t k = 0; k < N; ++k)
+            fptr[k] = use_bf16 ? (const void *)Ab[k].ptr : (const void *)A[k];
+        for (uint32_t m = 0; m < N; ++m) {
+            for (uint32_t i = 0; i < N; ++i) order[i] = (m + i) % N;
+            PTI_TRY(mttkrp_device(t, fptr.data(), use_bf16 ? PTI_B200_BF16 : PTI_B200_F32, R, stride, order.data(), m,
+                                  M.as<float>(), s));
+            gram_inverse_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), work.as<double>(), flag);
+            PTI_CUDA(cudaMemsetAsync(stats.ptr, 0, (size_t)R * 12, s), mod);
+            solve_rows_kernel<<<rows_grid((uint64_t)t->ndims[m] * stride, 256), 256, solve_smem, s>>>(
+                M.as<float>(), W.as<double>(), t->ndims[m], R, stride, A[m], colsq, colmax);
+            lambda_kernel<<<1, 128, 0, s>>>(colsq, colmax, R, it == 0, lambda);
+            PTI_CUDA(cudaMemsetAsync(G.as<double>() + (size_t)m * RR, 0, (size_t)RR * 8, s), mod);
+            gram_kernel<<<rows_grid(t->ndims[m], 32), 256, gram_smem, s>>>(
+                A[m], t->ndims[m], R, stride, lambda, mixed ? Ab[m].as<__nv_bfloat16>() : nullptr,
+                G.as<double>() + (size_t)m * RR);
+            PTI_CUDA(cudaGetLastError(), mod);
+        }
+        const uint32_t last = N - 1;
+        PTI_CUDA(cudaMemsetAsync(inner, 0, 8, s), mod);
+        inner_kernel<<<rows_grid((uint64_t)t->ndims[last] * stride, 256), 256, 0, s>>>(
+            A[last], M.as<float>(), t->ndims[last], R, stride, lambda, inner);
+        fit_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, lambda, normX2, inner, fits + it);
+        PTI_CUDA(cudaGetLastError(), mod);
+        if (opt.tol > 0.0) {
+            double fit = 0.0;
+            PTI_CUDA(cudaMemcpyAsync(&fit, fits + it, 8, cudaMemcpyDeviceToHost, s), mod);
+            PTI_CUDA(cudaStreamSynchronize(s), mod);
+            // cpd.c:144: stop when the fit changes by less than tol
+            if (it > 0 && std::fabs(fit - oldfit) < opt.tol) {
+                ++it;
+                break;
+            }
+            oldfit = fit;
+        }
+    }
+    res.iters = it;
+    // GetFinalLambda (matrix.c:556-572)
+    for (uint32_t m = 0; m < N; ++m) {
+        PTI_CUDA(cudaMemsetAsync(colsq, 0, (size_t)R * 8, s), mod);
+        colsq_kernel<<<rows_grid((uint64_t)t->ndims[m] * stride, 256), 256, R * 8, s>>>(A[m], t->ndims[m], R, stride,
+                                                                                        colsq);
+        final_scale_kernel<<<rows_grid((uint64_t)t->ndims[m] * stride, 256), 256, 0, s>>>(A[m], t->ndims[m], R,
+                                                                                          stride, colsq, lambda, 1);
+    }
+    PTI_CUDA(cudaGetLastError(), mod);
+    res.fits.resize(it);
+    int hflag = 0;
+    if (it) PTI_CUDA(cudaMemcpyAsync(res.fits.data(), fits, it * 8, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    res.solver_flags = hflag;
+    return 0;
+}
+
+int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
+int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s);
+int take_device_error(cudaStream_t s, const char *mod);
+
+namespace {
+
+// Runs CPD-ALS on an uploaded tensor from the reference's initial factors
+// (A[i][j] = i + j + 1, src/matrix/matrix.c:67-74) and copies the result into
+// host rows (stride floats each) through `sink(m, device_ptr)`.
+template <class Sink>
+int host_cpd(ptiB200Tensor *t, uint32_t R, uint32_t niters, double tol, float *lambda_host, double *fit_out,
+             Sink sink, cudaStream_t s)
+{
+    const char *mod = "B200 CPD-ALS";
+    const uint32_t N = t->nmodes;
+    const uint32_t stride = ((R - 1) / 8 + 1) * 8;
+    DevBuf A[kMaxModes], lam;
+    float *ptrs[kMaxModes];
+    for (uint32_t m = 0; m < N; ++m) {
+        const size_t n = (size_t)t->ndims[m] * stride;
+        std::vector<float> h(n, 0.f);
+        for (uint32_t i = 0; i < t->ndims[m]; ++i)
+            for (uint32_t j = 0; j < R; ++j) h[(size_t)i * stride + j] = (float)(i + j + 1);
+        PTI_CUDA(A[m].alloc(padded(n * 4), s), mod);
+        PTI_CUDA(cudaMemcpyAsync(A[m].ptr, h.data(), n * 4, cudaMemcpyHostToDevice, s), mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+        ptrs[m] = A[m].as<float>();
+    }
+    PTI_CUDA(lam.alloc(padded(R * 4), s), mod);
+    CpdOptions opt;
+    opt.R = R;
+    opt.niters = niters;
+    opt.tol = tol;
+    CpdResult res;
+    PTI_TRY(cpd_device(t, ptrs, stride, lam.as<float>(), opt, res, s));
+    PTI_CUDA(cudaMemcpyAsync(lambda_host, lam.ptr, R * 4, cudaMemcpyDeviceToHost, s), mod);
+    for (uint32_t m = 0; m < N; ++m) PTI_TRY(sink(m, A[m].as<float>(), stride));
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    *fit_out = res.iters ? res.fits.back() : 0.0;
+    return 0;
+}
+
+int cpd_coo_entry(const ptiSparseTensor *X, ptiIndex R, ptiIndex niters, double tol, ptiKruskalTensor *k)
+{
+    const char *mod = "B200 CPD-ALS";
+    PTI_CHECK(X && k && k->lambda, PTIERR_VALUE_ERROR, mod, "null tensor or Kruskal tensor");
+    PTI_CHECK(R >= 1, PTIERR_VALUE_ERROR, mod, "rank must be positive");
+    cudaStream_t s = sync_stream();
+    ptiB200Tensor t;
+    PTI_TRY(upload_coo(&t, X, s));
+    const uint32_t N = X->nmodes;
+    ptiMatrix **mats = static_cast<ptiMatrix **>(std::calloc(N + 1, sizeof(ptiMatrix *)));
+    for (uint32_t m = 0; m <= N; ++m) mats[m] = static_cast<ptiMatrix *>(std::calloc(1, sizeof(ptiMatrix)));
+    for (uint32_t m = 0; m < N; ++m) PTI_TRY(ptiNewMatrix(mats[m], X->ndims[m], R));
+    auto sink = [&](uint32_t m, const float *d, uint32_t stride) -> int {
+        PTI_CUDA(cudaMemcpyAsync(mats[m]->values, d, (size_t)X->ndims[m] * stride * 4, cudaMemcpyDeviceToHost, s),
+                 mod);
+        return 0;
+    };
+    double fit = 0.0;
+    int r = host_cpd(&t, R, niters, tol, k->lambda, &fit, sink, s);
+    if (r) {
+        for (uint32_t m = 0; m <= N; ++m) {
+            if (m < N) ptiFreeMatrix(mats[m]);
+            std::free(mats[m]);
+        }
+        std::free(mats);
+        return r;
+    }
+    // ktensor->factors = mats with mats[N] released (cpd.c:200-205)
+    k->factors = mats;
+    k->fit = fit;
+    return 0;
+}
+
+int cpd_hicoo_entry(const ptiSparseTensorHiCOO *H, ptiIndex R, ptiIndex niters, double tol, ptiRankKruskalTensor *k)
+{
+    const char *mod = "B200 HiCOO CPD-ALS";
+    PTI_CHECK(H && k && k->lambda, PTIERR_VALUE_ERROR, mod, "null tensor or Kruskal tensor");
+    PTI_CHECK(R >= 1 && R <= 248, PTIERR_VALUE_ERROR, mod, "rank must be in [1, 248] for ptiRankMatrix");
+    cudaStream_t s = sync_stream();
+    ptiB200Tensor t;
+    PTI_TRY(upload_hicoo(&t, H, s));
+    const uint32_t N = H->nmodes;
+    ptiRankMatrix **mats = static_cast<ptiRankMatrix **>(std::calloc(N + 1, sizeof(ptiRankMatrix *)));
+    for (uint32_t m = 0; m <= N; ++m) mats[m] = static_cast<ptiRankMatrix *>(std::calloc(1, sizeof(ptiRankMatrix)));
+    for (uint32_t m = 0; m < N; ++m) PTI_TRY(ptiNewRankMatrix(mats[m], H->ndims[m], (ptiElementIndex)R));
+    auto sink = [&](uint32_t m, const float *d, uint32_t stride) -> int {
+        PTI_CUDA(cudaMemcpyAsync(mats[m]->values, d, (size_t)H->ndims[m] * stride * 4, cudaMemcpyDeviceToHost, s),
+                 mod);
+        return 0;
+    };
+    double fit = 0.0;
+    int r = host_cpd(&t, R, niters, tol, k->lambda, &fit, sink, s);
+    if (r) {
+        for (uint32_t m = 0; m <= N; ++m) {
+            if (m < N) ptiFreeRankMatrix(mats[m]);
+            std::free(mats[m]);
+        }
+        std::free(mats);
+        return r;
+    }
+    k->factors = mats;
+    k->fit = fit;
+    return 0;
+}
+
+}  // namespace
+}  // namespace pti
+
+extern "C" {
+
+int ptiCpdAls(ptiSparseTensor const *const ptien, ptiIndex const rank, ptiIndex const niters, double const tol,
+              ptiKruskalTensor *ktensor)
+{
+    return pti::cpd_coo_entry(ptien, rank, niters, tol, ktensor);
+}
+int ptiOmpCpdAls(ptiSparseTensor const *const ptien, ptiIndex const rank, ptiIndex const niters, double const tol,
+                 const int tk, const int use_reduce, ptiKruskalTensor *ktensor)
+{
+    (void)tk;
+    (void)use_reduce;
+    return pti::cpd_coo_entry(ptien, rank, niters, tol, ktensor);
+}
+int ptiCudaCpdAls(ptiSparseTensor const *const ptien, ptiIndex const rank, ptiIndex const niters, double const tol,
+                  ptiKruskalTensor *ktensor)
+{
+    return pti::cpd_coo_entry(ptien, rank, niters, tol, ktensor);
+}
+int ptiCpdAlsHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiIndex const rank, ptiIndex const niters,
+                   double const tol, ptiRankKruskalTensor *ktensor)
+{
+    return pti::cpd_hicoo_entry(hitsr, rank, niters, tol, ktensor);
+}
+int ptiOmpCpdAlsHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiIndex const rank, ptiIndex const niters,
+                      double const tol, const int tk, const int tb, int balanced, ptiRankKruskalTensor *ktensor)
+{
+    (void)tk;
+    (void)tb;
+    (void)balanced;
+    return pti::cpd_hicoo_entry(hitsr, rank, niters, tol, ktensor);
+}
+
+int ptiB200CpdAls(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, int precision, ptiIndex fp32_sweeps,
+                  float *const *dev_factors, ptiIndex stride, float *dev_lambda, double *fits, ptiIndex *iters_done,
+                  void *stream)
+{
+    using namespace pti;
+    PTI_CHECK(t && dev_factors && dev_lambda, PTIERR_VALUE_ERROR, "B200 CPD-ALS", "null argument");
+    CpdOptions opt;
+    opt.R = rank;
+    opt.niters = niters;
+    opt.tol = tol;
+    opt.precision = precision;
+    opt.fp32_sweeps = fp32_sweeps;
+    CpdResult res;
+    PTI_TRY(cpd_device(t, dev_factors, stride, dev_lambda, opt, res, static_cast<cudaStream_t>(stream)));
+    if (fits)
+        for (uint32_t i = 0; i < res.iters; ++i) fits[i] = res.fits[i];
+    if (iters_done) *iters_done = res.iters;
+    return 0;
+}
+
+double SparseTensorFrobeniusNormSquared(ptiSparseTensor const *const ptien)
+{
+    using namespace pti;
+    if (!ptien || ptien->nnz == 0) return 0.0;
+    cudaStream_t s = sync_stream();
+    DevBuf v, acc;
+    double h = 0.0;
+    if (v.alloc(padded(ptien->nnz * 4), s) != cudaSuccess || acc.alloc(64, s) != cudaSuccess) return -1.0;
+    cudaMemcpyAsync(v.ptr, ptien->values.data, ptien->nnz * 4, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(acc.ptr, 0, 8, s);
+    sumsq_kernel<<<(unsigned)std::min<uint64_t>((ptien->nnz + 255) / 256, (uint64_t)sm_count() * 8), 256, 0, s>>>(
+        v.as<float>(), ptien->nnz, acc.as<double>());
+    cudaMemcpyAsync(&h, acc.ptr, 8, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+}
+
+}  // extern "C"

@@ -576,6 +576,22 @@ int ptiB200FreeTensor(ptiB200Tensor *t)
     return 0;
 }
 
+int ptiB200DownloadHiCOO(ptiB200Tensor const *t, ptiNnzIndex *bptr, void *const *binds, void *const *einds,
+                         ptiValue *vals)
+{
+    const char *mod = "B200 Download";
+    PTI_CHECK(t && t->hicoo && bptr && binds && einds && vals, PTIERR_VALUE_ERROR, mod, "need a HiCOO handle");
+    cudaStream_t s = pti::sync_stream();
+    PTI_CUDA(cudaMemcpyAsync(bptr, t->bptr.ptr, (t->nb + 1) * 8, cudaMemcpyDeviceToHost, s), mod);
+    for (uint32_t m = 0; m < t->nmodes; ++m) {
+        if (t->nb) PTI_CUDA(cudaMemcpyAsync(binds[m], t->binds[m].ptr, t->nb * 4, cudaMemcpyDeviceToHost, s), mod);
+        if (t->nnz) PTI_CUDA(cudaMemcpyAsync(einds[m], t->einds[m].ptr, t->nnz, cudaMemcpyDeviceToHost, s), mod);
+    }
+    if (t->nnz) PTI_CUDA(cudaMemcpyAsync(vals, t->vals.ptr, t->nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
 int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndims_out)
 {
     PTI_CHECK(t && info, PTIERR_VALUE_ERROR, "B200 Info", "null argument");

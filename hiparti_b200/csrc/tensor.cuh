@@ -62,10 +62,6 @@ struct ptiB200Tensor {
 
 namespace pti {
 
-// Allocation sizes are rounded up to 64 bytes plus one 64-byte guard so that
-// vectorised and bulk copies of a final partial tile stay inside the buffer.
-inline size_t padded(size_t bytes) { return ((bytes + 63) / 64) * 64 + 64; }
-
 int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
 int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s);
 

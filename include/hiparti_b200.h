@@ -265,6 +265,10 @@ int ptiB200ConvertToHiCOO(ptiB200Tensor **out, ptiB200Tensor *coo, ptiElementInd
 /* Build the per-mode schedule for `mode` now (otherwise built on first use). */
 int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream);
 int ptiB200FreeTensor(ptiB200Tensor *t);
+/* Copies a device HiCOO tensor's arrays to host buffers: bptr (nb+1),
+ * binds[m] (nb each), einds[m] (nnz each), vals (nnz).  Synchronous. */
+int ptiB200DownloadHiCOO(ptiB200Tensor const *t, ptiNnzIndex *bptr, void * const *binds,
+                         void * const *einds, ptiValue *vals);
 /* Shape and statistics of a device tensor.  info: [nmodes, nnz, nb, sb, sk, sc, is_hicoo]. */
 int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndims_out);
 
@@ -275,6 +279,18 @@ int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndi
 int ptiB200MTTKRP(ptiB200Tensor *t, const void * const *dev_mats, int factor_type, ptiIndex rank,
                   ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode, float *dev_out,
                   void *stream);
+
+/* CPD-ALS with everything in device memory.  dev_factors[k] (ndims[k] x stride
+ * FP32, stride a multiple of 8) hold the initial factors and receive the
+ * result; dev_lambda (rank floats) receives the weights.  precision selects
+ * the factor copy the MTTKRP gathers read: PTI_B200_F32, or PTI_B200_BF16 for
+ * all but the last fp32_sweeps iterations.  Grams, solves and fits are FP64.
+ * fits (host, niters doubles, may be NULL) receives the fit after every
+ * iteration; iters_done the number of iterations run (tol > 0 stops early as
+ * in src/sptensor/cpd.c:144).  rank <= 128.  Synchronous on `stream`. */
+int ptiB200CpdAls(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, int precision,
+                  ptiIndex fp32_sweeps, float * const *dev_factors, ptiIndex stride, float *dev_lambda,
+                  double *fits, ptiIndex *iters_done, void *stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

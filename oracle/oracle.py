@@ -314,6 +314,20 @@ class Ref:
                 v = h.kschr[m][i]
                 rows.append(_np_from(v.data, int(v.len), np.uint32))
         res["kschr_rows"] = rows
+        # balanced scheduler (convert.c:475-571)
+        kb = C.cast(h.kschr_balanced, C.POINTER(C.POINTER(_Vec)))
+        kp = C.cast(h.kschr_balanced_pos, C.POINTER(C.POINTER(_Vec)))
+        kr = C.cast(h.kschr_rest, C.POINTER(_Vec))
+        bal, pos, rest = [], [], []
+        for m in range(N):
+            for i in range((int(dims[m]) + (1 << sk) - 1) >> sk):
+                bal.append(_np_from(kb[m][i].data, int(kb[m][i].len), np.uint32))
+                pos.append(_np_from(kp[m][i].data, int(kp[m][i].len), np.uint32))
+            rest.append(_np_from(kr[m].data, int(kr[m].len), np.uint32))
+        res["kschr_balanced_rows"] = bal
+        res["kschr_balanced_pos_rows"] = pos
+        res["kschr_rest"] = rest
+        res["nkpars"] = _np_from(h.nkpars, N, np.uint32)
         self.L.ptiFreeSparseTensorHiCOO(C.byref(h))
         return res
 

@@ -1,0 +1,123 @@
+"""CPU: the C-ABI library loads, exports every entry point the header declares,
+lays out the reference's structs byte for byte, and runs its host-side logic
+(containers, the .tns/.bin reader, argument checks) without a GPU."""
+import re
+import struct
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from hiparti_b200 import COOTensor, HiCOOTensor, PtiError, ffi, synth
+
+HEADER = ROOT / "include" / "hiparti_b200.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    names = re.findall(r"^\s*(?:int|void|double)\s+\**\s*(\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    import subprocess
+    so = ROOT / "hiparti_b200" / "libhiparti_b200.so"
+    out = subprocess.run(["nm", "-D", "--defined-only", str(so)], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    names = declared_functions()
+    assert len(names) >= 40
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        getattr(lib, n)  # cffi resolves each declared symbol
+
+
+def test_struct_layout_matches_reference():
+    # sizes/offsets of include/includes/structs.h compiled with the reference
+    # headers on x86-64 (gcc): see the reference struct definitions.
+    assert ffi.sizeof("ptiSparseTensorHiCOO") == 224
+    assert ffi.sizeof("ptiSparseTensor") == 64
+    assert ffi.sizeof("ptiMatrix") == 24
+    assert ffi.sizeof("ptiRankMatrix") == 24
+    assert ffi.sizeof("ptiKruskalTensor") == 40
+    assert ffi.sizeof("ptiRankKruskalTensor") == 40
+    off = {"sb_bits": 32, "kptr": 40, "kschr": 64, "cptr": 80, "knnzs": 136, "bptr": 160,
+           "binds": 184, "einds": 192, "values": 200}
+    for f, o in off.items():
+        assert ffi.offsetof("ptiSparseTensorHiCOO", f) == o, f
+    assert ffi.offsetof("ptiRankMatrix", "stride") == 12
+    assert ffi.offsetof("ptiKruskalTensor", "fit") == 24
+    assert ffi.offsetof("ptiSparseTensor", "values") == 40
+
+
+def test_matrix_life_cycle(lib):
+    m = ffi.new("ptiMatrix *")
+    assert lib.ptiNewMatrix(m, 5, 11) == 0
+    assert (m.nrows, m.ncols, m.cap, m.stride) == (5, 11, 5, 16)
+    assert int(ffi.cast("uintptr_t", m.values)) % 32 == 0
+    assert lib.ptiRandomizeMatrix(m) == 0
+    assert m.values[2 * 16 + 3] == 6.0  # i + j + 1
+    assert lib.ptiConstantMatrix(m, 2.5) == 0
+    assert m.values[4 * 16 + 10] == 2.5
+    lib.ptiFreeMatrix(m)
+
+
+def test_load_tns_and_bin(lib, tmp_path):
+    p = tmp_path / "t.tns"
+    p.write_text("3\n4 5 6\n1 1 1 1.5\n4 5 6 -2.0\n2 3 1 0.25\n")
+    t = COOTensor.load(str(p))
+    assert t.dims == [4, 5, 6] and t.nnz == 3
+    np.testing.assert_array_equal(t.inds[0], [0, 3, 1])
+    np.testing.assert_array_equal(t.inds[2], [0, 5, 0])
+    np.testing.assert_array_equal(t.vals, np.float32([1.5, -2.0, 0.25]))
+    # SPLATT binary: header, nmodes, dims, nnz, indices per mode, values
+    b = tmp_path / "t.bin"
+    with open(b, "wb") as f:
+        f.write(struct.pack("<iQQ", 0, 4, 4))
+        f.write(struct.pack("<I", 3) + struct.pack("<3I", 4, 5, 6) + struct.pack("<I", 2))
+        f.write(struct.pack("<2I", 0, 3) + struct.pack("<2I", 1, 4) + struct.pack("<2I", 5, 0))
+        f.write(struct.pack("<2f", 1.0, 2.0))
+    tb = COOTensor.load(str(b))
+    assert tb.dims == [4, 5, 6]
+    np.testing.assert_array_equal(tb.inds[1], [1, 4])
+    np.testing.assert_array_equal(tb.vals, np.float32([1, 2]))
+
+
+def test_load_reference_fixture_if_present(lib):
+    from pathlib import Path
+    f = Path("/root/reference/data/tensors/3d_7.tns")
+    if not f.exists():
+        pytest.skip("reference data not mounted")
+    t = COOTensor.load(str(f))
+    assert t.nmodes == 3 and t.nnz == 9
+
+
+def test_shape_mismatch_is_reported_before_any_gpu_work(lib):
+    dims = (5, 6, 7)
+    coo = COOTensor(dims, [np.array([1], np.uint32)] * 3, np.array([1.0], np.float32))
+    mats = synth.factor_matrices((5, 6, 8), 8, seed=1)
+    with pytest.raises(PtiError) as e:
+        coo.mttkrp(mats, 8, 0)
+    assert e.value.code == 2
+    code = lib.ptiGetLastError(ffi.NULL, ffi.NULL, ffi.NULL, ffi.NULL)
+    assert code == 2
+    lib.ptiClearLastError()
+    assert lib.ptiGetLastError(ffi.NULL, ffi.NULL, ffi.NULL, ffi.NULL) == 0
+
+
+def test_conversion_argument_checks(lib):
+    dims = (5, 6)
+    coo = COOTensor(dims, [np.array([1], np.uint32)] * 2, np.array([1.0], np.float32))
+    with pytest.raises(PtiError) as e:
+        coo.to_hicoo(2, 3, 3)  # 2-D: the reference has no Morton order for it
+    assert e.value.code == 3
+    with pytest.raises(PtiError) as e:
+        COOTensor((5, 6, 7), [np.array([1], np.uint32)] * 3, np.array([1.0], np.float32)).to_hicoo(4, 3, 5)
+    assert e.value.code == 3
+
+
+def test_hicoo_struct_round_trip(lib):
+    h = HiCOOTensor((4, 4, 4), 1, 2, 2, np.array([0, 2], np.uint64), [np.array([1], np.uint32)] * 3,
+                    [np.array([0, 1], np.uint8)] * 3, np.array([1, 2], np.float32))
+    assert h.nb == 1 and h.nnz == 2
+    assert h.c.bptr.len == 2 and h.c.binds[0].data[0] == 1
