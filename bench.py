@@ -153,15 +153,15 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def make_c2(device, seed):
+def make_c2(device, seed, nnz=C2_NNZ):
     """C2 tensor on the device: torch COO -> device HiCOO (GPU conversion)."""
     import torch
     from hiparti_b200 import DeviceTensor
     from hiparti_b200.synth import coords_torch
-    inds = coords_torch(C2_DIMS, C2_NNZ, seed, zipf_s=1.1, device=device)
+    inds = coords_torch(C2_DIMS, nnz, seed, zipf_s=1.1, device=device)
     g = torch.Generator(device=device)
     g.manual_seed(seed + 1)
-    vals = torch.rand(C2_NNZ, generator=g, device=device, dtype=torch.float32)
+    vals = torch.rand(nnz, generator=g, device=device, dtype=torch.float32)
     coo = DeviceTensor.from_torch_coo(C2_DIMS, inds, vals)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -183,13 +183,20 @@ def run_ours_mttkrp(args, rank, world):
     import torch
     from hiparti_b200 import HiCOOTensor, ffi, lib
     dev = torch.device("cuda", torch.cuda.current_device())
-    coo, h, inds, vals, conv_s = make_c2(dev, SEED + rank)
+    nnz = args.nnz
+    coo, h, inds, vals, conv_s = make_c2(dev, SEED + rank, nnz)
     nb = h.nb
     mats = c2_factors(dev, SEED + rank)
     stride = mats[0].shape[1]
     N = 3
+    # per-mode schedules (built once per tensor, reused by every MTTKRP)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h.prepare()
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
     outs = [torch.empty((d, stride), dtype=torch.float32, device=dev) for d in C2_DIMS]
-    bytes_mode = [hicoo_bytes(C2_NNZ, nb, C2_DIMS, C2_R, N) for _ in range(N)]
+    bytes_mode = [hicoo_bytes(nnz, nb, C2_DIMS, C2_R, N) for _ in range(N)]
     step_bytes = sum(bytes_mode)
     stream = torch.cuda.current_stream()
 
@@ -233,7 +240,7 @@ def run_ours_mttkrp(args, rank, world):
 
     # ---- end to end through the reference-facing C ABI (host buffers) ----
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         e2e = run_e2e(h, inds, vals, mats, nb, args)
 
     result = {
@@ -241,9 +248,9 @@ def run_ours_mttkrp(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Zipf(1.1) coordinates, U(0,1) values and factors)",
-        "config": {"workload": "C2 HiCOO MTTKRP, 3-D 200000x150000x20000, 50M nnz Zipf(1.1), R=32, "
-                               "sb=7 sk=10 sc=14, FP32, all 3 modes per step",
-                   "nnz": C2_NNZ, "nb": nb, "rank": C2_R, "modes_per_step": N,
+        "config": {"workload": f"C2 HiCOO MTTKRP, 3-D 200000x150000x20000, {nnz // 1000000}M nnz Zipf(1.1), "
+                               "R=32, sb=7 sk=10 sc=14, FP32, all 3 modes per step",
+                   "nnz": nnz, "nb": nb, "prepare_s": round(prep_s, 3), "rank": C2_R, "modes_per_step": N,
                    "algorithmic_bytes_per_step": step_bytes,
                    "l2": "inputs larger than L2 (tensor 0.8 GB vs 126 MB L2)",
                    "parallelism": f"replicas x{world}", "conversion_s": round(conv_s, 3),
@@ -308,7 +315,7 @@ def run_e2e(h_dev, inds, vals, mats, nb, args):
     fac_bytes = [m.nbytes for m in hmats]
     h2d = sum(tensor_bytes + sum(fac_bytes) - fac_bytes[m] for m in range(N))
     d2h = sum(C2_DIMS[m] * stride * 4 for m in range(N))
-    step_bytes = N * hicoo_bytes(C2_NNZ, nb, C2_DIMS, C2_R, N)
+    step_bytes = N * hicoo_bytes(host["vals"].size, nb, C2_DIMS, C2_R, N)
     return {"value": round(step_bytes / dt / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": round(dt * 1e3, 3), "steps": ksteps,
             "api": "ptiMTTKRPHiCOO (C ABI, host pinned buffers, tensor + factors copied in per call)"}
@@ -399,6 +406,9 @@ def main():
     ap.add_argument("--workload", default="mttkrp", choices=["mttkrp"])
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nnz", type=int, default=C2_NNZ,
+                    help="nonzeros of the C2 construction (smaller only for profiling captures)")
     args = ap.parse_args()
 
     if args.impl == "reference":

@@ -429,6 +429,7 @@ int alloc_element_vector(ptiElementIndexVector *v, uint64_t len);
 int alloc_value_vector(ptiValueVector *v, uint64_t len);
 int alloc_nnz_vector(ptiNnzIndexVector *v, uint64_t len);
 int balanced_schedule(ptiSparseTensorHiCOO *hitsr, uint64_t nnz);
+int validate_coo(ptiB200Tensor *t, cudaStream_t s);
 
 }  // namespace pti
 
@@ -537,6 +538,11 @@ int ptiB200TensorFromDeviceCOO(ptiB200Tensor **out, ptiIndex nmodes, const ptiIn
     if (r) {
         delete t;
         PTI_FAIL(r, mod, "device copy failed");
+    }
+    r = validate_coo(t, s);
+    if (r) {
+        delete t;
+        return r;
     }
     *out = t;
     return 0;

@@ -149,13 +149,14 @@ __global__ void check_coo_kernel(const uint32_t *ind, uint64_t nnz, uint32_t dim
         if (ind[z] >= dim) atomicOr(err, 1u);
 }
 
-// bptr must start at 0, end at nnz and never decrease.
+// bptr must start at 0, end at nnz and increase strictly (no empty blocks:
+// the kernels size their per-tile block tables by that).
 __global__ void check_bptr_kernel(const uint64_t *bptr, uint64_t nb, uint64_t nnz, uint32_t *err)
 {
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= nb;
          b += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t v = bptr[b];
-        if ((b == 0 && v != 0) || (b == nb && v != nnz) || (b < nb && bptr[b + 1] < v) || v > nnz)
+        if ((b == 0 && v != 0) || (b == nb && v != nnz) || (b < nb && bptr[b + 1] <= v) || v > nnz)
             atomicOr(err, 1u);
     }
 }
@@ -210,6 +211,21 @@ void launch_hicoo(const HicooArgs &a, int G, unsigned ntiles, cudaStream_t s)
 
 int ensure_err_word(cudaStream_t s);
 uint32_t *err_word();
+int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
+                     const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
+bool schedule_supported(const ptiB200Tensor *t, uint32_t R);
+
+// The output-privatised kernels (sched.cu) cover orders 2-4 and R <= 128;
+// HIPARTI_B200_SCHEDULE=0 selects the direct-atomic kernels instead.
+static bool use_schedule(const ptiB200Tensor *t, uint32_t R)
+{
+    static int env = -1;
+    if (env < 0) {
+        const char *e = std::getenv("HIPARTI_B200_SCHEDULE");
+        env = (e && e[0] == '0') ? 0 : 1;
+    }
+    return env == 1 && schedule_supported(t, R);
+}
 
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                   const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s)
@@ -239,6 +255,10 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     PTI_CUDA(cudaMemsetAsync(out, 0, (size_t)t->ndims[mode] * stride * sizeof(float), s), mod);
     if (t->nnz == 0) return 0;
     const int G = group_lanes(R);
+    if (use_schedule(t, R)) {
+        PTI_TRY(prepare_mode(t, mode, s));
+        return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s);
+    }
 
     if (!t->hicoo) {
         CooArgs a{};
@@ -352,6 +372,21 @@ int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s)
     PTI_TRY(ensure_err_word(s));
     if (t->nnz) {
         for (uint32_t m = 0; m < X->nmodes; ++m)
+            check_coo_kernel<<<grid_for(t->nnz, 256), 256, 0, s>>>(t->inds[m].as<uint32_t>(), t->nnz,
+                                                                   t->ndims[m], err_word());
+        PTI_CUDA(cudaGetLastError(), mod);
+        PTI_TRY(take_device_error(s, mod));
+    }
+    return 0;
+}
+
+// Checks every index of a device COO tensor against the mode sizes.
+int validate_coo(ptiB200Tensor *t, cudaStream_t s)
+{
+    const char *mod = "B200 Upload";
+    PTI_TRY(ensure_err_word(s));
+    if (t->nnz) {
+        for (uint32_t m = 0; m < t->nmodes; ++m)
             check_coo_kernel<<<grid_for(t->nnz, 256), 256, 0, s>>>(t->inds[m].as<uint32_t>(), t->nnz,
                                                                    t->ndims[m], err_word());
         PTI_CUDA(cudaGetLastError(), mod);
@@ -617,10 +652,8 @@ int ptiB200MTTKRP(ptiB200Tensor *t, const void *const *dev_mats, int factor_type
 
 int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream)
 {
-    (void)t;
-    (void)mode;
-    (void)stream;
-    return 0;
+    PTI_CHECK(t, PTIERR_VALUE_ERROR, "B200 Prepare", "null handle");
+    return pti::prepare_mode(t, mode, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -129,7 +129,7 @@ constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // keys per CTA, striped
 constexpr int kSortWarps = kSortThreads / 32;
 
-__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t *keys, uint64_t n, int shift,
+static __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t *keys, uint64_t n, int shift,
                                                                   uint32_t ntiles, uint32_t *hist)
 {
     __shared__ uint32_t s_hist[256];
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s_hist[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t *keys_in, const uint32_t *vals_in,
+static __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t *keys_in, const uint32_t *vals_in,
                                                                      uint64_t n, int shift, uint32_t ntiles,
                                                                      const uint32_t *offsets, uint64_t *keys_out,
                                                                      uint32_t *vals_out)

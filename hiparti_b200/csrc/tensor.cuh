@@ -27,11 +27,11 @@ struct HicooModePlan {
     uint32_t ntiles = 0;
 };
 
-// Per-mode schedule of a COO tensor: nonzeros sorted by the output-mode index.
+// Per-mode schedule of a COO tensor: nonzeros sorted by the output-mode index,
+// packed as 16- or 32-byte records {out index, operand indices, value}.
 struct CooModePlan {
     bool ready = false;
-    std::array<DevBuf, kMaxModes> inds;   // uint32 [nnz]
-    DevBuf vals;                          // float [nnz]
+    DevBuf recs;                          // uint32 [nnz][4 or 8]
 };
 
 }  // namespace pti
