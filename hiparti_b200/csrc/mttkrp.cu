@@ -11,6 +11,8 @@
 #include "kutil.cuh"
 #include "tensor.cuh"
 
+#include <mutex>
+
 namespace pti {
 
 constexpr int kThreads = 256;
@@ -97,10 +99,16 @@ __global__ void __launch_bounds__(kThreads) hicoo_tile_kernel(HicooArgs a)
     const uint64_t z0 = (uint64_t)blockIdx.x * kHiTile;
     const uint64_t z1 = min(z0 + kHiTile, a.nnz);
     const uint32_t b0 = a.tile_block[blockIdx.x];
+    if (b0 >= a.nb) {  // only a malformed bptr leaves a tile without a block
+        if (threadIdx.x == 0) atomicOr(a.err, 1u);
+        return;
+    }
     uint32_t nblk = a.tile_block[blockIdx.x + 1] - b0 + 1;
     if (nblk > kHiTile + 1) nblk = kHiTile + 1;
     if (b0 + (uint64_t)nblk > a.nb) nblk = (uint32_t)(a.nb - b0);
 
+    for (uint32_t z = threadIdx.x; z < kHiTile; z += kThreads) s_blk[z] = 0;
+    __syncthreads();
     for (uint32_t i = threadIdx.x; i < nblk; i += kThreads) {
         const uint64_t b = b0 + i;
         s_out[i] = __ldg(a.out_bind + b) << a.sb;
@@ -657,3 +665,122 @@ int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// HiCOO MTTKRP that allocates nothing.
+//
+// Some callers cannot allocate device memory while they run this operation:
+// code inside a host framework that owns every byte of device memory through
+// its own pool, services with a fixed memory budget that must not grow or fail
+// mid-request, and real-time loops where a cudaMalloc would block.  This entry
+// point therefore keeps its only scratch -- the tile-to-block table the kernel
+// needs and the error word -- in fixed arrays in device global memory that are
+// part of the library image.  Every GPU that loads the library holds them
+// (about 1 MiB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace pti {
+namespace {
+
+constexpr uint32_t kNoAllocMaxTiles = 1u << 18;  // tiles of kHiTile nonzeros: up to 268,435,456 nonzeros
+
+static __device__ __align__(256) uint32_t g_noalloc_tile_block[kNoAllocMaxTiles + 1];
+static __device__ __align__(256) uint32_t g_noalloc_err[64];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocScratch {
+    uint32_t *tile_block;
+    uint32_t *err;
+};
+NoAllocScratch g_noalloc_scratch[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Device addresses of the scratch arrays for the current device, looked up
+// once per device (host code must not use the symbols' host-side names as
+// device pointers).
+int noalloc_scratch(NoAllocScratch &out, const char *mod)
+{
+    int dev = 0;
+    PTI_CUDA(cudaGetDevice(&dev), mod);
+    PTI_CHECK(dev >= 0 && dev < kNoAllocMaxDevices, PTIERR_VALUE_ERROR, mod, "device ordinal too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocScratch &sc = g_noalloc_scratch[dev];
+    if (!sc.tile_block) {
+        void *tb = nullptr, *er = nullptr;
+        PTI_CUDA(cudaGetSymbolAddress(&tb, g_noalloc_tile_block), mod);
+        PTI_CUDA(cudaGetSymbolAddress(&er, g_noalloc_err), mod);
+        sc.err = static_cast<uint32_t *>(er);
+        sc.tile_block = static_cast<uint32_t *>(tb);
+    }
+    out = sc;
+    return 0;
+}
+
+}  // namespace
+}  // namespace pti
+
+extern "C" int ptiB200MTTKRPHiCOONoAlloc(ptiIndex nmodes, const ptiIndex *ndims, ptiNnzIndex nnz, ptiNnzIndex nb,
+                                         ptiElementIndex sb_bits, const ptiNnzIndex *dev_bptr,
+                                         const ptiBlockIndex *const *dev_binds,
+                                         const ptiElementIndex *const *dev_einds, const ptiValue *dev_vals,
+                                         const float *const *dev_mats, ptiIndex rank, ptiIndex stride,
+                                         const ptiIndex *mats_order, ptiIndex mode, float *dev_out, void *stream)
+{
+    using namespace pti;
+    const char *mod = "B200 HiCOO MTTKRP (no allocation)";
+    PTI_CHECK(ndims && mats_order && dev_mats && dev_out, PTIERR_VALUE_ERROR, mod, "null argument");
+    PTI_CHECK(nmodes >= 2 && nmodes <= (uint32_t)kMaxModes, PTIERR_VALUE_ERROR, mod, "unsupported number of modes");
+    PTI_CHECK(mode < nmodes, PTIERR_VALUE_ERROR, mod, "mode out of range");
+    PTI_CHECK(sb_bits <= 8, PTIERR_VALUE_ERROR, mod, "sb_bits must be <= 8");
+    PTI_CHECK(rank >= 1 && stride >= rank && stride % 4 == 0, PTIERR_SHAPE_MISMATCH, mod,
+              "stride must be >= rank and a multiple of 4");
+    const uint64_t ntiles = (nnz + kHiTile - 1) / kHiTile;
+    PTI_CHECK(ntiles <= kNoAllocMaxTiles, PTIERR_VALUE_ERROR, mod,
+              "more than 268,435,456 nonzeros: beyond the fixed scratch of this entry point");
+    PTI_CHECK(nnz == 0 || (nb >= 1 && nb < 0xFFFFFFFFull && dev_bptr && dev_binds && dev_einds && dev_vals),
+              PTIERR_VALUE_ERROR, mod, "missing HiCOO arrays");
+    uint32_t seen = 0;
+    for (uint32_t i = 0; i < nmodes; ++i) {
+        PTI_CHECK(mats_order[i] < nmodes && !(seen >> mats_order[i] & 1u), PTIERR_VALUE_ERROR, mod,
+                  "mats_order must be a permutation of the modes");
+        seen |= 1u << mats_order[i];
+    }
+    PTI_CHECK(mats_order[0] == mode, PTIERR_VALUE_ERROR, mod, "mats_order[0] must equal mode");
+    PTI_CHECK(((uintptr_t)dev_out & 15) == 0, PTIERR_VALUE_ERROR, mod, "output must be 16-byte aligned");
+    for (uint32_t i = 1; i < nmodes; ++i)
+        PTI_CHECK(dev_mats[mats_order[i]] && ((uintptr_t)dev_mats[mats_order[i]] & 15) == 0, PTIERR_VALUE_ERROR,
+                  mod, "factors must be non-null and 16-byte aligned");
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NoAllocScratch sc;
+    PTI_TRY(noalloc_scratch(sc, mod));
+    PTI_CUDA(cudaMemsetAsync(dev_out, 0, (size_t)ndims[mode] * stride * sizeof(float), s), mod);
+    PTI_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(uint32_t), s), mod);
+    if (nnz == 0) return 0;
+
+    tile_block_kernel<<<ceil_div(nb, 256), 256, 0, s>>>(dev_bptr, nb, (uint32_t)ntiles, sc.tile_block);
+    HicooArgs a{};
+    a.nnz = nnz;
+    a.nb = nb;
+    a.nin = nmodes - 1;
+    a.R = rank;
+    a.stride = stride;
+    a.sb = sb_bits;
+    a.bptr = dev_bptr;
+    a.tile_block = sc.tile_block;
+    a.out_bind = dev_binds[mode];
+    a.out_eind = dev_einds[mode];
+    a.out_dim = ndims[mode];
+    for (uint32_t i = 1; i < nmodes; ++i) {
+        const uint32_t k = mats_order[i];
+        a.in_bind[i - 1] = dev_binds[k];
+        a.in_eind[i - 1] = dev_einds[k];
+        a.in_dim[i - 1] = ndims[k];
+        a.in_mat[i - 1] = dev_mats[k];
+    }
+    a.vals = dev_vals;
+    a.out = dev_out;
+    a.err = sc.err;
+    launch_hicoo<float>(a, group_lanes(rank), (unsigned)ntiles, s);
+    PTI_CUDA(cudaGetLastError(), mod);
+    return 0;
+}

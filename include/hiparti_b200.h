@@ -280,6 +280,31 @@ int ptiB200MTTKRP(ptiB200Tensor *t, const void * const *dev_mats, int factor_typ
                   ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode, float *dev_out,
                   void *stream);
 
+/* HiCOO MTTKRP that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc while it runs: code
+ * whose device memory is owned by a host framework's pool, services with a
+ * fixed memory budget, real-time loops where an allocation could block.  The
+ * caller passes the HiCOO arrays (bptr nb+1, binds[m] nb each, einds[m] and
+ * vals nnz each; bptr strictly increasing), the FP32 factors (ndims[k] x
+ * stride, 16-byte aligned) and the output (ndims[mode] x stride), all in
+ * device memory; ndims, mats_order and the pointer arrays live in host memory.
+ * The kernel's scratch (a tile table and an error word) sits in fixed arrays
+ * in the library's device image -- about 1 MiB that every GPU which loads the
+ * library keeps until exit -- which limits nnz to 268,435,456 (2^18 tiles of
+ * 1024); larger tensors are rejected with PTIERR_VALUE_ERROR.  The first call
+ * on a device looks up the arrays' device addresses, so make that first call
+ * before any stream capture.  All calls share the scratch: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be ordered by
+ * the caller.  Runs asynchronously on `stream`; out-of-range coordinates are
+ * skipped, not reported.  Uses the direct-atomic kernel (no per-mode schedule,
+ * which would need memory). */
+int ptiB200MTTKRPHiCOONoAlloc(ptiIndex nmodes, const ptiIndex *ndims, ptiNnzIndex nnz, ptiNnzIndex nb,
+                              ptiElementIndex sb_bits, const ptiNnzIndex *dev_bptr,
+                              const ptiBlockIndex * const *dev_binds,
+                              const ptiElementIndex * const *dev_einds, const ptiValue *dev_vals,
+                              const float * const *dev_mats, ptiIndex rank, ptiIndex stride,
+                              const ptiIndex *mats_order, ptiIndex mode, float *dev_out, void *stream);
+
 /* CPD-ALS with everything in device memory.  dev_factors[k] (ndims[k] x stride
  * FP32, stride a multiple of 8) hold the initial factors and receive the
  * result; dev_lambda (rank floats) receives the weights.  precision selects
