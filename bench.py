@@ -179,6 +179,82 @@ def c2_factors(device, seed):
     return [torch.rand((d, stride), generator=g, device=device, dtype=torch.float32) for d in C2_DIMS]
 
 
+def make_c3(device, seed):
+    """C3: 4-D 20000^3 x 500, 40M unique uniform coordinates; values of a
+    planted rank-10 Kruskal model (|N(0,1)| entries, unit-norm columns,
+    weights U(1,10)) plus N(0, 0.01^2) noise (0.01 read as the standard
+    deviation)."""
+    import torch
+    from hiparti_b200.synth import coords_torch
+    inds = coords_torch(C3_DIMS, C3_NNZ, seed, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 3)
+    rank = 10
+    lam = torch.rand(rank, generator=g, device=device, dtype=torch.float64) * 9 + 1
+    model = lam.expand(C3_NNZ, rank).clone()
+    for d, ix in zip(C3_DIMS, inds):
+        a = torch.randn((d, rank), generator=g, device=device, dtype=torch.float64).abs_()
+        a /= a.norm(dim=0, keepdim=True)
+        model *= a[ix.long()]
+    noise = torch.randn(C3_NNZ, generator=g, device=device, dtype=torch.float64) * 0.01
+    vals = (model.sum(1) + noise).float()
+    del model, noise
+    return inds, vals
+
+
+def run_cpd(args):
+    """C3 CPD-ALS: FP32 factors vs BF16 factors for the MTTKRP gathers (FP32
+    accumulation, FP64 Grams/solves; the last fp32_sweeps iterations in FP32),
+    same start; final fits against the FP64 oracle from the same start."""
+    import torch
+    from hiparti_b200 import DeviceTensor
+    dev = torch.device("cuda", torch.cuda.current_device())
+    inds, vals = make_c3(dev, SEED + 7)
+    coo = DeviceTensor.from_torch_coo(C3_DIMS, inds, vals)
+    t = coo.to_hicoo(7, 10, 14) if args.cpd_format == "hicoo" else coo
+    t.prepare()
+    stride = ((C3_R - 1) // 8 + 1) * 8
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 8)
+    init = [torch.rand((d, stride), generator=g, device=dev, dtype=torch.float32) for d in C3_DIMS]
+    for a in init:
+        a[:, C3_R:] = 0
+    out = {"workload": f"C3 CPD-ALS: 4-D 20000^3x500, 40M nnz planted rank-10 + N(0,0.01^2), R={C3_R}, "
+                       f"{args.cpd_iters} iterations, {args.cpd_format.upper()} tensor",
+           "iters": args.cpd_iters, "fp32_sweeps": args.fp32_sweeps}
+    results = {}
+    for prec in ["fp32", "bf16"]:
+        # one warm-up iteration, then the timed run from the same start
+        fac = [a.clone() for a in init]
+        t.cpd_als(fac, 1, rank=C3_R, precision=prec, fp32_sweeps=1 if prec == "fp32" else 0)
+        fac = [a.clone() for a in init]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lam, fits = t.cpd_als(fac, args.cpd_iters, rank=C3_R, precision=prec,
+                              fp32_sweeps=args.fp32_sweeps if prec == "bf16" else args.cpd_iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        results[prec] = (dt / args.cpd_iters, fits[-1])
+        out[f"s_per_iter_{prec}"] = round(dt / args.cpd_iters, 6)
+        out[f"fit_{prec}"] = fits[-1]
+    out["speedup_bf16_vs_fp32"] = round(results["fp32"][0] / results["bf16"][0], 3)
+    if args.cpd_oracle:
+        from oracle.oracle import Orc, ensure_built
+        ensure_built(ref=False)
+        orc = Orc()
+        t0 = time.perf_counter()
+        o = orc.cpd_als(list(C3_DIMS), [i.cpu().numpy().astype(np.uint32) for i in inds], vals.cpu().numpy(),
+                        C3_R, args.cpd_iters, [a[:, :C3_R].cpu().numpy() for a in init])
+        out["fit_fp64_oracle"] = o["fit"]
+        out["oracle_s"] = round(time.perf_counter() - t0, 1)
+        out["fit_diff_fp32"] = abs(results["fp32"][1] - o["fit"])
+        out["fit_diff_bf16"] = abs(results["bf16"][1] - o["fit"])
+    coo.free()
+    if t is not coo:
+        t.free()
+    return out
+
+
 def run_ours_mttkrp(args, rank, world):
     import torch
     from hiparti_b200 import HiCOOTensor, ffi, lib
@@ -257,7 +333,7 @@ def run_ours_mttkrp(args, rank, world):
                    "per_mode_ms": [round(x, 4) for x in per_mode_ms]},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "hicoo_tile_kernel (per-mode launch)",
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "hicoo_sched_kernel (one launch per mode)",
                      "mean_launch_ms": round(mean_launch_ms, 4)},
         "clocks": clocks,
         "e2e": e2e,
@@ -407,6 +483,11 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpd", action="store_true", help="skip the CPD-ALS (C3) block")
+    ap.add_argument("--cpd-iters", type=int, default=C3_ITERS)
+    ap.add_argument("--cpd-format", default="hicoo", choices=["hicoo", "coo"])
+    ap.add_argument("--fp32-sweeps", type=int, default=2)
+    ap.add_argument("--cpd-oracle", type=int, default=1)
     ap.add_argument("--nnz", type=int, default=C2_NNZ,
                     help="nonzeros of the C2 construction (smaller only for profiling captures)")
     args = ap.parse_args()
@@ -426,6 +507,10 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_block(args)
+        if world == 1 and not args.no_cpd:
+            import torch
+            torch.cuda.empty_cache()
+            res["cpd"] = run_cpd(args)
         print(json.dumps(res), flush=True)
     if world > 1:
         import torch.distributed as dist

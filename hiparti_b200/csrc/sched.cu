@@ -63,79 +63,68 @@ struct Rec {
     static constexpr int words = ((NIN + 2 + 3) / 4) * 4;
 };
 
-// Columns of one operand row held by a lane: V float4 (FP32) or, for BF16, the
-// same 4V values from one 8V-byte load.
-template <int V>
-struct Cols {
-    float2 x[2 * V];
-};
-
-template <int V>
-__device__ __forceinline__ void load_cols(Cols<V> &c, const float *row, uint32_t col)
-{
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-        const float4 f = __ldg(reinterpret_cast<const float4 *>(row + col) + q);
-        c.x[2 * q] = make_float2(f.x, f.y);
-        c.x[2 * q + 1] = make_float2(f.z, f.w);
-    }
-}
-
-template <int V>
-__device__ __forceinline__ void load_cols(Cols<V> &c, const __nv_bfloat16 *row, uint32_t col)
-{
-    if constexpr (V == 2) {
-        const uint4 r = __ldg(reinterpret_cast<const uint4 *>(row + col));
-        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) c.x[q] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w[q]));
-    } else {
-        const uint2 r = __ldg(reinterpret_cast<const uint2 *>(row + col));
-        c.x[0] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.x));
-        c.x[1] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.y));
-    }
-}
-
-template <int V>
-__device__ __forceinline__ void flush_cols(float *out_row, uint32_t col, uint32_t R, const Cols<V> &acc)
-{
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-        const uint32_t c = col + 4 * q;
-        if (c < R) {
-            float4 v = make_float4(acc.x[2 * q].x, acc.x[2 * q].y, acc.x[2 * q + 1].x, acc.x[2 * q + 1].y);
-            red_add4(out_row + c, mask4(v, c, R));
+// Columns of one operand row held by a lane: 4 (one float4 of FP32) or 8 (one
+// 16-byte load of BF16).
+template <int CPL, class FT>
+struct RowPart {
+    uint4 raw;
+    __device__ __forceinline__ void load(const FT *row, uint32_t col)
+    {
+        if constexpr (CPL == 4 && sizeof(FT) == 4) {
+            const float4 f = __ldg(reinterpret_cast<const float4 *>(row + col));
+            raw = make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z), __float_as_uint(f.w));
+        } else if constexpr (CPL == 8) {
+            raw = __ldg(reinterpret_cast<const uint4 *>(row + col));
+        } else {
+            const uint2 r = __ldg(reinterpret_cast<const uint2 *>(row + col));
+            raw = make_uint4(r.x, r.y, 0u, 0u);
         }
     }
-}
+    // column c (0 <= c < CPL) as FP32
+    __device__ __forceinline__ float at(int c) const
+    {
+        const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
+        if constexpr (sizeof(FT) == 4) {
+            return __uint_as_float(w[c]);
+        } else {
+            const uint32_t h = w[c >> 1];
+            return __uint_as_float((c & 1) ? (h & 0xFFFF0000u) : (h << 16));
+        }
+    }
+};
 
 // Walks records [j0, j1) (ordered by output row): gathers the operand rows,
-// accumulates v * prod_k A_k[row_k] in registers (FP32x2), and adds the sum
-// into the output once per run of equal output rows.
-template <int G, int V, int U, int NIN, class FT>
+// accumulates v * prod_k A_k[row_k] in registers, and adds the sum into the
+// output once per run of equal output rows.
+template <int G, int CPL, int U, int NIN, class FT>
 __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t j0, uint32_t j1, uint32_t lane,
                                                 const SchedArgs &a)
 {
     constexpr int RW = Rec<NIN>::words;
-    const uint32_t col = lane * 4 * V;
+    const uint32_t col = lane * CPL;
     const bool active = col < a.R;
-    Cols<V> acc;
+    float acc[CPL];
 #pragma unroll
-    for (int q = 0; q < 2 * V; ++q) acc.x[q] = make_float2(0.f, 0.f);
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
     uint32_t cur = 0xFFFFFFFFu;
+    auto flush = [&](uint32_t row) {
+#pragma unroll
+        for (int q = 0; q < CPL / 4; ++q)
+            if (col + 4 * q < a.R)
+                red_add4(a.out + (size_t)row * a.stride + col + 4 * q,
+                         mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]), col + 4 * q, a.R));
+    };
     for (uint32_t j = j0; j < j1; j += U) {
         uint32_t orow[U];
         float val[U];
-        Cols<V> f[U][NIN];
+        RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             orow[u] = 0xFFFFFFFFu;
             if (j + u < j1) {
-                const uint4 r0 = *reinterpret_cast<const uint4 *>(s_rec + (size_t)(j + u) * RW);
                 uint32_t w[RW];
-                w[0] = r0.x; w[1] = r0.y; w[2] = r0.z; w[3] = r0.w;
 #pragma unroll
-                for (int q = 4; q < RW; q += 4) {
+                for (int q = 0; q < RW; q += 4) {
                     const uint4 r = *reinterpret_cast<const uint4 *>(s_rec + (size_t)(j + u) * RW + q);
                     w[q] = r.x; w[q + 1] = r.y; w[q + 2] = r.z; w[q + 3] = r.w;
                 }
@@ -144,7 +133,7 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
                 if (orow[u] != 0xFFFFFFFFu && active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
-                        load_cols<V>(f[u][k], static_cast<const FT *>(a.in_mat[k]) + (size_t)w[1 + k] * a.stride, col);
+                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)w[1 + k] * a.stride, col);
                 }
             }
         }
@@ -152,24 +141,23 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
         for (int u = 0; u < U; ++u) {
             if (orow[u] == 0xFFFFFFFFu) continue;
             if (orow[u] != cur) {
-                if (cur != 0xFFFFFFFFu && active) flush_cols<V>(a.out + (size_t)cur * a.stride, col, a.R, acc);
+                if (cur != 0xFFFFFFFFu && active) flush(cur);
 #pragma unroll
-                for (int q = 0; q < 2 * V; ++q) acc.x[q] = make_float2(0.f, 0.f);
+                for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
                 cur = orow[u];
             }
             if (active) {
-                const float2 vv = make_float2(val[u], val[u]);
 #pragma unroll
-                for (int q = 0; q < 2 * V; ++q) {
-                    float2 p = __fmul2_rn(vv, f[u][0].x[q]);
+                for (int c = 0; c < CPL; ++c) {
+                    float p = val[u] * f[u][0].at(c);
 #pragma unroll
-                    for (int k = 1; k < NIN - 1; ++k) p = __fmul2_rn(p, f[u][k].x[q]);
-                    acc.x[q] = NIN > 1 ? __ffma2_rn(p, f[u][NIN - 1].x[q], acc.x[q]) : __fadd2_rn(acc.x[q], p);
+                    for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
+                    acc[c] += p;
                 }
             }
         }
     }
-    if (cur != 0xFFFFFFFFu && active) flush_cols<V>(a.out + (size_t)cur * a.stride, col, a.R, acc);
+    if (cur != 0xFFFFFFFFu && active) flush(cur);
 }
 
 template <int NIN>
@@ -186,7 +174,7 @@ struct HiSmem {
     static constexpr uint32_t total = bin + 4 * NIN * (kHiTile + 4);
 };
 
-template <int G, class FT, int NIN>
+template <int G, int CPL, class FT, int NIN>
 __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 {
     using L = HiSmem<NIN>;
@@ -245,7 +233,7 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
-    const uint32_t col = lane * 4;
+    const uint32_t col = lane * CPL;
     const bool active = col < a.R;
     const uint32_t span = (uint32_t)kHist >> a.sb;
     uint32_t zs = 0;
@@ -298,14 +286,24 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         __syncthreads();
 
         // each group: a contiguous run of the row-sorted nonzeros
-        const uint32_t cnt = ze - zs, per = (cnt + kGroups - 1) / kGroups;
+        // an odd slice length puts the groups' first records on different shared-memory banks
+        const uint32_t cnt = ze - zs, per = ((cnt + kGroups - 1) / kGroups) | 1u;
         const uint32_t j0 = min(zs + g * per, ze), j1 = min(j0 + per, ze);
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        float acc[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
         uint32_t cur = 0xFFFFFFFFu;
+        auto flush = [&](uint32_t row) {
+#pragma unroll
+            for (int q = 0; q < CPL / 4; ++q)
+                if (col + 4 * q < a.R)
+                    red_add4(a.out + (size_t)row * a.stride + col + 4 * q,
+                             mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]), col + 4 * q, a.R));
+        };
         for (uint32_t j = j0; j < j1; j += U) {
             uint32_t orow[U];
             float v[U];
-            float4 f[U][NIN];
+            RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 orow[u] = 0xFFFFFFFFu;
@@ -328,33 +326,37 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
                 if (active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
-                        f[u][k] = load4(static_cast<const FT *>(a.in_mat[k]) + (size_t)r[k] * a.stride, col);
+                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)r[k] * a.stride, col);
                 }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (orow[u] == 0xFFFFFFFFu) continue;
                 if (orow[u] != cur) {
-                    if (cur != 0xFFFFFFFFu && active) red_add4(a.out + (size_t)cur * a.stride + col, mask4(acc, col, a.R));
-                    acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (cur != 0xFFFFFFFFu && active) flush(cur);
+#pragma unroll
+                    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
                     cur = orow[u];
                 }
                 if (active) {
-                    float4 p = scale4(f[u][0], v[u]);
 #pragma unroll
-                    for (int k = 1; k < NIN; ++k) p = mul4(p, f[u][k]);
-                    acc = add4(acc, p);
+                    for (int c = 0; c < CPL; ++c) {
+                        float p = v[u] * f[u][0].at(c);
+#pragma unroll
+                        for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
+                        acc[c] += p;
+                    }
                 }
             }
         }
-        if (cur != 0xFFFFFFFFu && active) red_add4(a.out + (size_t)cur * a.stride + col, mask4(acc, col, a.R));
+        if (cur != 0xFFFFFFFFu && active) flush(cur);
         __syncthreads();
         zs = ze;
     }
 }
 
 // COO schedule: packed records sorted by output index; no sorting in the kernel.
-template <int G, int V, int U, int MINB, class FT, int NIN>
+template <int G, int CPL, int U, int MINB, class FT, int NIN>
 __global__ void __launch_bounds__(kSchedThreads, MINB) coo_sched_kernel(SchedArgs a, const uint32_t *recs)
 {
     constexpr int RW = Rec<NIN>::words;
@@ -384,9 +386,9 @@ __global__ void __launch_bounds__(kSchedThreads, MINB) coo_sched_kernel(SchedArg
     }
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
-    const uint32_t per = (n + kGroups - 1) / kGroups;
+    const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;  // odd: groups start on different banks
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
-    process_records<G, V, U, NIN, FT>(s_rec, j0, j1, lane, a);
+    process_records<G, CPL, U, NIN, FT>(s_rec, j0, j1, lane, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -592,56 +594,75 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // Launch
 // ---------------------------------------------------------------------------
-template <int G, int V, int U, class FT, int NIN>
+template <int G, int CPL, int U, class FT, int NIN>
 static int launch_coo(const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = (size_t)kTile * Rec<NIN>::words * 4;
-    auto k = coo_sched_kernel<G, V, U, 4, FT, NIN>;
+    auto k = coo_sched_kernel<G, CPL, U, 4, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a, recs);
     return 0;
 }
 
-template <int G, class FT, int NIN>
+template <int G, int CPL, class FT, int NIN>
 static int launch_hicoo(const SchedArgs &a, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = HiSmem<NIN>::total;
-    auto k = hicoo_sched_kernel<G, FT, NIN>;
+    auto k = hicoo_sched_kernel<G, CPL, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a);
     return 0;
 }
 
-// Lanes per nonzero: one float4 of columns per lane, one column pass (R <= 128).
+// Lanes per nonzero: 4 columns per lane (FP32 factors, or BF16 factors that
+// are not 16-byte addressable by rows) or 8 columns per lane (BF16 with a
+// stride that is a multiple of 8); one column pass (R <= 128).
 template <class FT, int NIN>
-static int launch_r(bool hicoo, const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
+static int launch_r(bool hicoo, bool wide, const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
 {
     const uint32_t R = a.R;
-    if (hicoo) {
-        if (R <= 4) return launch_hicoo<1, FT, NIN>(a, ntiles, s);
-        if (R <= 8) return launch_hicoo<2, FT, NIN>(a, ntiles, s);
-        if (R <= 16) return launch_hicoo<4, FT, NIN>(a, ntiles, s);
-        if (R <= 32) return launch_hicoo<8, FT, NIN>(a, ntiles, s);
-        if (R <= 64) return launch_hicoo<16, FT, NIN>(a, ntiles, s);
-        return launch_hicoo<32, FT, NIN>(a, ntiles, s);
+    if constexpr (sizeof(FT) == 2) {
+        if (wide) {
+            if (hicoo) {
+                if (R <= 8) return launch_hicoo<1, 8, FT, NIN>(a, ntiles, s);
+                if (R <= 16) return launch_hicoo<2, 8, FT, NIN>(a, ntiles, s);
+                if (R <= 32) return launch_hicoo<4, 8, FT, NIN>(a, ntiles, s);
+                if (R <= 64) return launch_hicoo<8, 8, FT, NIN>(a, ntiles, s);
+                return launch_hicoo<16, 8, FT, NIN>(a, ntiles, s);
+            }
+            if (R <= 8) return launch_coo<1, 8, 2, FT, NIN>(a, recs, ntiles, s);
+            if (R <= 16) return launch_coo<2, 8, 2, FT, NIN>(a, recs, ntiles, s);
+            if (R <= 32) return launch_coo<4, 8, 2, FT, NIN>(a, recs, ntiles, s);
+            if (R <= 64) return launch_coo<8, 8, 2, FT, NIN>(a, recs, ntiles, s);
+            return launch_coo<16, 8, 2, FT, NIN>(a, recs, ntiles, s);
+        }
     }
-    if (R <= 4) return launch_coo<1, 1, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 8) return launch_coo<2, 1, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 16) return launch_coo<4, 1, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 32) return launch_coo<8, 1, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 64) return launch_coo<16, 1, 2, FT, NIN>(a, recs, ntiles, s);
-    return launch_coo<32, 1, 2, FT, NIN>(a, recs, ntiles, s);
+    if (hicoo) {
+        if (R <= 4) return launch_hicoo<1, 4, FT, NIN>(a, ntiles, s);
+        if (R <= 8) return launch_hicoo<2, 4, FT, NIN>(a, ntiles, s);
+        if (R <= 16) return launch_hicoo<4, 4, FT, NIN>(a, ntiles, s);
+        if (R <= 32) return launch_hicoo<8, 4, FT, NIN>(a, ntiles, s);
+        if (R <= 64) return launch_hicoo<16, 4, FT, NIN>(a, ntiles, s);
+        return launch_hicoo<32, 4, FT, NIN>(a, ntiles, s);
+    }
+    if (R <= 4) return launch_coo<1, 4, 3, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 8) return launch_coo<2, 4, 3, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 16) return launch_coo<4, 4, 3, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 32) return launch_coo<8, 4, 3, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 64) return launch_coo<16, 4, 2, FT, NIN>(a, recs, ntiles, s);
+    return launch_coo<32, 4, 2, FT, NIN>(a, recs, ntiles, s);
 }
 
 template <class FT>
-static int launch_n(int nin, bool hicoo, const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
+static int launch_n(int nin, bool hicoo, bool wide, const SchedArgs &a, const uint32_t *recs, unsigned ntiles,
+                    cudaStream_t s)
 {
     switch (nin) {
-        case 1: return launch_r<FT, 1>(hicoo, a, recs, ntiles, s);
-        case 2: return launch_r<FT, 2>(hicoo, a, recs, ntiles, s);
-        default: return launch_r<FT, 3>(hicoo, a, recs, ntiles, s);
+        case 1: return launch_r<FT, 1>(hicoo, wide, a, recs, ntiles, s);
+        case 2: return launch_r<FT, 2>(hicoo, wide, a, recs, ntiles, s);
+        default: return launch_r<FT, 3>(hicoo, wide, a, recs, ntiles, s);
     }
 }
 
@@ -695,8 +716,13 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
                 ++i;
             }
     }
-    int r = ft == PTI_B200_F32 ? launch_n<float>((int)N - 1, t->hicoo, a, recs, ntiles, s)
-                               : launch_n<__nv_bfloat16>((int)N - 1, t->hicoo, a, recs, ntiles, s);
+    // BF16 rows are read 8 columns (16 bytes) per lane when every row start
+    // is 16-byte aligned.
+    bool wide = ft == PTI_B200_BF16 && stride % 8 == 0;
+    for (uint32_t k = 0; k < N && wide; ++k)
+        if (k != mode && ((uintptr_t)mats[k] & 15) != 0) wide = false;
+    int r = ft == PTI_B200_F32 ? launch_n<float>((int)N - 1, t->hicoo, false, a, recs, ntiles, s)
+                               : launch_n<__nv_bfloat16>((int)N - 1, t->hicoo, wide, a, recs, ntiles, s);
     PTI_CHECK(r == 0, r, mod, "kernel attribute setup failed");
     PTI_CUDA(cudaGetLastError(), mod);
     return 0;

@@ -43,19 +43,30 @@ void orc_mttkrp_coo_f64(uint32_t nmodes, uint64_t nnz, const uint32_t *const *in
                         const float *vals, const double *const *mats, uint32_t R,
                         uint32_t stride, uint32_t mode, uint32_t out_rows, double *out)
 {
-    memset(out, 0, (size_t)out_rows * stride * sizeof(double));
-    double *scratch = (double *)malloc((R ? R : 1) * sizeof(double));
-    for (uint64_t x = 0; x < nnz; ++x) {
-        for (uint32_t r = 0; r < R; ++r) scratch[r] = (double)vals[x];
-        for (uint32_t k = 0; k < nmodes; ++k) {
-            if (k == mode) continue;
-            const double *row = mats[k] + (size_t)inds[k][x] * stride;
-            for (uint32_t r = 0; r < R; ++r) scratch[r] *= row[r];
+    /* OpenMP over nonzeros with thread-private outputs summed at the end, so
+     * the oracle finishes full-size CPD checks in seconds. */
+    const size_t len = (size_t)out_rows * stride;
+    memset(out, 0, len * sizeof(double));
+#pragma omp parallel
+    {
+        double *priv = (double *)calloc(len ? len : 1, sizeof(double));
+        double *scratch = (double *)malloc((R ? R : 1) * sizeof(double));
+#pragma omp for schedule(static)
+        for (uint64_t x = 0; x < nnz; ++x) {
+            for (uint32_t r = 0; r < R; ++r) scratch[r] = (double)vals[x];
+            for (uint32_t k = 0; k < nmodes; ++k) {
+                if (k == mode) continue;
+                const double *row = mats[k] + (size_t)inds[k][x] * stride;
+                for (uint32_t r = 0; r < R; ++r) scratch[r] *= row[r];
+            }
+            double *o = priv + (size_t)inds[mode][x] * stride;
+            for (uint32_t r = 0; r < R; ++r) o[r] += scratch[r];
         }
-        double *o = out + (size_t)inds[mode][x] * stride;
-        for (uint32_t r = 0; r < R; ++r) o[r] += scratch[r];
+#pragma omp critical
+        for (size_t i = 0; i < len; ++i) out[i] += priv[i];
+        free(priv);
+        free(scratch);
     }
-    free(scratch);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -522,6 +533,7 @@ double orc_kruskal_fit_f64(uint32_t nmodes, const uint32_t *ndims, uint64_t nnz,
     for (uint32_t p = 0; p < R; ++p)
         for (uint32_t q = 0; q < R; ++q) norm_mats += V[p * R + q] * lambda[p] * lambda[q];
     double normX2 = 0, inner = 0;
+#pragma omp parallel for reduction(+ : normX2, inner) schedule(static)
     for (uint64_t z = 0; z < nnz; ++z) {
         double model = 0;
         for (uint32_t r = 0; r < R; ++r) {
