@@ -255,6 +255,60 @@ def run_cpd(args):
     return out
 
 
+C4_DIMS = (100_000, 100_000, 100_000)
+C4_NNZ = 20_000_000
+C4_R = 64
+
+
+def run_gradcp(args):
+    """C4 gradient CP: 100,000^3, 20M uniform nonzeros, values of a planted
+    rank-16 model (|N(0,1)| entries, unit-norm columns, weights U(1,10)) plus
+    N(0, 0.05^2) noise; R=64 FP32 factors N(0, 0.1).  One step = loss
+    0.5*sum (x - model)^2 at the nonzeros + backward (3 residual MTTKRPs)."""
+    import torch
+    from hiparti_b200 import DeviceTensor
+    from hiparti_b200.autograd import cp_loss
+    from hiparti_b200.synth import coords_torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    inds = coords_torch(C4_DIMS, C4_NNZ, SEED + 11, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 12)
+    lam = torch.rand(16, generator=g, device=dev, dtype=torch.float64) * 9 + 1
+    model = lam.expand(C4_NNZ, 16).clone()
+    for d, ix in zip(C4_DIMS, inds):
+        a = torch.randn((d, 16), generator=g, device=dev, dtype=torch.float64).abs_()
+        a /= a.norm(dim=0, keepdim=True)
+        model *= a[ix.long()]
+    vals = (model.sum(1) + 0.05 * torch.randn(C4_NNZ, generator=g, device=dev, dtype=torch.float64)).float()
+    del model
+    dt = DeviceTensor.from_torch_coo(C4_DIMS, inds, vals)
+    dt.prepare()
+    stride = C4_R
+    facs = [(0.1 * torch.randn((d, stride), generator=g, device=dev)).requires_grad_(True) for d in C4_DIMS]
+
+    def step():
+        for f in facs:
+            f.grad = None
+        loss = cp_loss(dt, vals, facs, rank=C4_R)
+        loss.backward()
+        return loss
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = 5
+    e0.record()
+    for _ in range(k):
+        loss = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    dt.free()
+    return {"workload": "C4 gradient CP: 100000^3, 20M nnz planted rank-16 + N(0,0.05^2), R=64 FP32, "
+                        "loss + backward (model at nonzeros + 3 residual MTTKRPs)",
+            "ms_per_gradient": round(ms, 3), "loss": float(loss.item())}
+
+
 def run_ours_mttkrp(args, rank, world):
     import torch
     from hiparti_b200 import HiCOOTensor, ffi, lib
@@ -484,6 +538,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpd", action="store_true", help="skip the CPD-ALS (C3) block")
+    ap.add_argument("--no-gradcp", action="store_true", help="skip the gradient-CP (C4) block")
     ap.add_argument("--cpd-iters", type=int, default=C3_ITERS)
     ap.add_argument("--cpd-format", default="hicoo", choices=["hicoo", "coo"])
     ap.add_argument("--fp32-sweeps", type=int, default=2)
@@ -511,6 +566,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["cpd"] = run_cpd(args)
+        if world == 1 and not args.no_gradcp:
+            import torch
+            torch.cuda.empty_cache()
+            res["gradcp"] = run_gradcp(args)
         print(json.dumps(res), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -331,6 +331,35 @@ class DeviceTensor:
                                   mode, ffi.cast("float *", out.data_ptr()), stream), "ptiB200MTTKRP")
         return out
 
+    def kruskal_values(self, factors, rank=None, out=None):
+        """The CP model sum_r prod_k A_k[i_k, r] at every nonzero (input order)."""
+        import torch
+        stride = factors[0].shape[1]
+        R = stride if rank is None else int(rank)
+        if out is None:
+            out = torch.empty(self.info()["nnz"], dtype=torch.float32, device=factors[0].device)
+        fp = ffi.new("float *[]", [ffi.cast("float *", f.data_ptr()) for f in factors])
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200KruskalValues(self._h, fp, R, stride, ffi.cast("float *", out.data_ptr()), stream),
+              "ptiB200KruskalValues")
+        return out
+
+    def mttkrp_values(self, vals, factors, mode, rank=None, out=None):
+        """MTTKRP with the nonzero values replaced by `vals` (float32, input order)."""
+        import torch
+        N = len(self.dims)
+        stride = factors[0].shape[1]
+        R = stride if rank is None else int(rank)
+        if out is None:
+            out = torch.empty((self.dims[mode], stride), dtype=torch.float32, device=factors[0].device)
+        vals = vals.contiguous().to(torch.float32)
+        mp = ffi.new("void *[]", [ffi.cast("void *", f.data_ptr()) for f in factors])
+        order = ffi.new("ptiIndex[]", [(mode + i) % N for i in range(N)])
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200MTTKRPValues(self._h, ffi.cast("float *", vals.data_ptr()), mp, _F32, R, stride, order,
+                                        mode, ffi.cast("float *", out.data_ptr()), stream), "ptiB200MTTKRPValues")
+        return out
+
     def cpd_als(self, factors, niters, tol=0.0, precision="fp32", fp32_sweeps=1, rank=None):
         """CPD-ALS on the device (ptiB200CpdAls).  factors: list of float32 CUDA
         tensors (I_k, stride) holding the initial factors; updated in place.

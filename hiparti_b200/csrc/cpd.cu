@@ -304,9 +304,6 @@ __global__ void final_scale_kernel(float *A, uint32_t I, uint32_t R, uint32_t st
         for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) lambda[c] *= (float)sqrt(colsq[c]);
 }
 
-int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
-
 // ---------------------------------------------------------------------------
 // The ALS driver.
 // ---------------------------------------------------------------------------

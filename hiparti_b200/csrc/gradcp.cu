@@ -1,0 +1,115 @@
+// gradcp.cu -- the pieces of all-at-once gradient CP on a COO tensor:
+//   model(z) = sum_r prod_k A_k[i_k(z), r]     (the CP model at each nonzero)
+//   dL/dA_k  = MTTKRP_k(g)                     (g = dL/dmodel at the nonzeros)
+// For the loss 0.5 * sum_z (x_z - model(z))^2, g = model - x, so the gradient
+// of every factor is a per-mode MTTKRP of the residual; the Hadamard partials
+// are recomputed by the MTTKRP kernels rather than stored per nonzero.
+#include "kutil.cuh"
+#include "tensor.cuh"
+
+namespace pti {
+
+struct KVArgs {
+    uint64_t nnz;
+    uint32_t nmodes, R, stride;
+    const uint32_t *inds[kMaxModes];
+    const float *mats[kMaxModes];
+    float *out;
+};
+
+// A group of G lanes per nonzero; each lane multiplies 4 columns across the
+// modes and the group sums its lanes with shuffles.
+template <int G>
+__global__ void __launch_bounds__(256) kruskal_values_kernel(KVArgs a)
+{
+    constexpr uint32_t kGroupsPerWarp = 32 / G;
+    const uint32_t lane = threadIdx.x % G;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) / 32;
+    // the loop bound is uniform across a warp, so every lane reaches the shuffles
+    for (uint64_t base = warp * kGroupsPerWarp; base < a.nnz; base += nwarps * kGroupsPerWarp) {
+        const uint64_t z = base + (threadIdx.x % 32) / G;
+        const bool live = z < a.nnz;
+        float s = 0.f;
+        if (live) {
+            uint32_t rows[kMaxModes];
+#pragma unroll
+            for (int k = 0; k < kMaxModes; ++k)
+                if (k < (int)a.nmodes) rows[k] = __ldg(a.inds[k] + z);
+            for (uint32_t col = lane * 4; col < a.R; col += 4 * G) {
+                float4 p = load4(a.mats[0] + (size_t)rows[0] * a.stride, col);
+#pragma unroll
+                for (int k = 1; k < kMaxModes; ++k)
+                    if (k < (int)a.nmodes) p = mul4(p, load4(a.mats[k] + (size_t)rows[k] * a.stride, col));
+                p = mask4(p, col, a.R);
+                s += (p.x + p.y) + (p.z + p.w);
+            }
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+        if (live && lane == 0) a.out[z] = s;
+    }
+}
+
+static int lanes_for(uint32_t R)
+{
+    uint32_t q = (R + 3) / 4;
+    int g = 1;
+    while ((uint32_t)g < q && g < 32) g *= 2;
+    return g;
+}
+
+}  // namespace pti
+
+extern "C" {
+
+int ptiB200KruskalValues(ptiB200Tensor *t, const float *const *dev_factors, ptiIndex rank, ptiIndex stride,
+                         float *dev_out, void *stream)
+{
+    using namespace pti;
+    const char *mod = "B200 Kruskal values";
+    PTI_CHECK(t && dev_factors && dev_out, PTIERR_VALUE_ERROR, mod, "null argument");
+    PTI_CHECK(!t->hicoo, PTIERR_VALUE_ERROR, mod, "needs a COO tensor");
+    PTI_CHECK(rank >= 1 && stride >= rank && stride % 4 == 0, PTIERR_SHAPE_MISMATCH, mod,
+              "stride must be >= rank and a multiple of 4");
+    for (uint32_t k = 0; k < t->nmodes; ++k)
+        PTI_CHECK(dev_factors[k] && ((uintptr_t)dev_factors[k] & 15) == 0, PTIERR_VALUE_ERROR, mod,
+                  "factors must be non-null and 16-byte aligned");
+    if (t->nnz == 0) return 0;
+    KVArgs a{};
+    a.nnz = t->nnz;
+    a.nmodes = t->nmodes;
+    a.R = rank;
+    a.stride = stride;
+    for (uint32_t k = 0; k < t->nmodes; ++k) {
+        a.inds[k] = t->inds[k].as<uint32_t>();
+        a.mats[k] = dev_factors[k];
+    }
+    a.out = dev_out;
+    const int G = lanes_for(rank);
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((t->nnz * G + 255) / 256, (uint64_t)sm_count() * 16));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (G) {
+        case 1: kruskal_values_kernel<1><<<grid, 256, 0, s>>>(a); break;
+        case 2: kruskal_values_kernel<2><<<grid, 256, 0, s>>>(a); break;
+        case 4: kruskal_values_kernel<4><<<grid, 256, 0, s>>>(a); break;
+        case 8: kruskal_values_kernel<8><<<grid, 256, 0, s>>>(a); break;
+        case 16: kruskal_values_kernel<16><<<grid, 256, 0, s>>>(a); break;
+        default: kruskal_values_kernel<32><<<grid, 256, 0, s>>>(a); break;
+    }
+    PTI_CUDA(cudaGetLastError(), mod);
+    return 0;
+}
+
+int ptiB200MTTKRPValues(ptiB200Tensor *t, const float *dev_vals, const void *const *dev_mats, int factor_type,
+                        ptiIndex rank, ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode, float *dev_out,
+                        void *stream)
+{
+    PTI_CHECK(t && dev_vals && dev_mats && mats_order && dev_out, PTIERR_VALUE_ERROR, "B200 MTTKRP",
+              "null argument");
+    return pti::mttkrp_device(t, dev_mats, factor_type, rank, stride, mats_order, mode, dev_out,
+                              static_cast<cudaStream_t>(stream), dev_vals);
+}
+
+}  // extern "C"

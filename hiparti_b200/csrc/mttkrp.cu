@@ -220,7 +220,8 @@ void launch_hicoo(const HicooArgs &a, int G, unsigned ntiles, cudaStream_t s)
 int ensure_err_word(cudaStream_t s);
 uint32_t *err_word();
 int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                     const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
+                     const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
+                     const float *vals_override);
 bool schedule_supported(const ptiB200Tensor *t, uint32_t R);
 
 // The output-privatised kernels (sched.cu) cover orders 2-4 and R <= 128;
@@ -236,7 +237,7 @@ static bool use_schedule(const ptiB200Tensor *t, uint32_t R)
 }
 
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s)
+                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s, const float *vals_override)
 {
     const char *mod = "B200 MTTKRP";
     const uint32_t N = t->nmodes;
@@ -254,6 +255,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
         seen |= 1u << mats_order[i];
     }
     PTI_CHECK(mats_order[0] == mode, PTIERR_VALUE_ERROR, mod, "mats_order[0] must equal mode");
+    PTI_CHECK(!vals_override || !t->hicoo, PTIERR_VALUE_ERROR, mod, "substituted values need a COO tensor");
     const size_t esz = ft == PTI_B200_F32 ? 4 : 2;
     for (uint32_t i = 1; i < N; ++i) {
         PTI_CHECK(mats[mats_order[i]], PTIERR_VALUE_ERROR, mod, "null factor");
@@ -265,7 +267,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     const int G = group_lanes(R);
     if (use_schedule(t, R)) {
         PTI_TRY(prepare_mode(t, mode, s));
-        return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s);
+        return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s, vals_override);
     }
 
     if (!t->hicoo) {
@@ -279,7 +281,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
             a.in_ind[i - 1] = t->inds[mats_order[i]].as<uint32_t>();
             a.in_mat[i - 1] = mats[mats_order[i]];
         }
-        a.vals = t->vals.as<float>();
+        a.vals = vals_override ? vals_override : t->vals.as<float>();
         a.out = out;
         if (ft == PTI_B200_F32) launch_coo<float>(a, G, s);
         else launch_coo<__nv_bfloat16>(a, G, s);

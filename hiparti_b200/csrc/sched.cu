@@ -98,7 +98,7 @@ struct RowPart {
 // output once per run of equal output rows.
 template <int G, int CPL, int U, int NIN, class FT>
 __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t j0, uint32_t j1, uint32_t lane,
-                                                const SchedArgs &a)
+                                                const SchedArgs &a, const float *alt = nullptr)
 {
     constexpr int RW = Rec<NIN>::words;
     const uint32_t col = lane * CPL;
@@ -129,7 +129,7 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
                     w[q] = r.x; w[q + 1] = r.y; w[q + 2] = r.z; w[q + 3] = r.w;
                 }
                 orow[u] = w[0];
-                val[u] = __uint_as_float(w[1 + NIN]);
+                val[u] = alt ? __ldg(alt + j + u) : __uint_as_float(w[1 + NIN]);
                 if (orow[u] != 0xFFFFFFFFu && active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(kSchedThreads, MINB) coo_sched_kernel(SchedArg
     constexpr uint32_t kGroups = kSchedThreads / G;
     const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;  // odd: groups start on different banks
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
-    process_records<G, CPL, U, NIN, FT>(s_rec, j0, j1, lane, a);
+    process_records<G, CPL, U, NIN, FT>(s_rec, j0, j1, lane, a, a.vals ? a.vals + z0 : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -517,6 +517,7 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
         pa.vals = t->vals.as<float>();
         pack_records_kernel<<<grid_n(n), 256, 0, s>>>(pa, perm.as<uint32_t>(), n, P.recs.as<uint32_t>());
         PTI_CUDA(cudaGetLastError(), mod);
+        P.perm = std::move(perm);
         P.ready = true;
         return 0;
     }
@@ -674,7 +675,8 @@ bool schedule_supported(const ptiB200Tensor *t, uint32_t R)
 // Runs the scheduled kernel for `mode` (the schedule must be ready).  Output
 // must already be zeroed.
 int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                     const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s)
+                     const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
+                     const float *vals_override)
 {
     const char *mod = "B200 MTTKRP";
     const uint32_t N = t->nmodes;
@@ -708,7 +710,14 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
     } else {
         // records hold the operand modes in increasing order
         ntiles = (unsigned)((t->nnz + kTile - 1) / kTile);
-        recs = t->coo_plan[mode].recs.as<uint32_t>();
+        CooModePlan &P = t->coo_plan[mode];
+        recs = P.recs.as<uint32_t>();
+        if (vals_override) {  // substituted values, brought into record order
+            if (!P.alt_vals.ptr) PTI_CUDA(P.alt_vals.alloc(padded(t->nnz * 4), s), mod);
+            gather_kernel<float><<<grid_n(t->nnz), 256, 0, s>>>(vals_override, P.perm.as<uint32_t>(), t->nnz,
+                                                                P.alt_vals.as<float>());
+            a.vals = P.alt_vals.as<float>();
+        }
         for (uint32_t k = 0, i = 0; k < N; ++k)
             if (k != mode) {
                 a.in_dim[i] = t->ndims[k];

@@ -32,6 +32,8 @@ struct HicooModePlan {
 struct CooModePlan {
     bool ready = false;
     DevBuf recs;                          // uint32 [nnz][4 or 8]
+    DevBuf perm;                          // uint32 [nnz]: record j holds input nonzero perm[j]
+    DevBuf alt_vals;                      // float [nnz]: caller-supplied values in record order
 };
 
 }  // namespace pti
@@ -66,8 +68,11 @@ int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
 int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s);
 
 // MTTKRP launchers; factors are device pointers (element type ft), out is FP32.
+// vals_override (optional): nnz values in the tensor's input order that replace
+// its own values (COO tensors only).
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s);
+                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
+                  const float *vals_override = nullptr);
 int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s);
 
 // Host-struct MTTKRP used by the reference entry points.

@@ -280,6 +280,18 @@ int ptiB200MTTKRP(ptiB200Tensor *t, const void * const *dev_mats, int factor_typ
                   ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode, float *dev_out,
                   void *stream);
 
+/* Gradient CP support (no reference counterpart), COO device tensors only.
+ * ptiB200KruskalValues: dev_out[z] = sum_r prod_k A_k[i_k(z), r] for every
+ * nonzero z in the tensor's input order (factors FP32, ndims[k] x stride).
+ * ptiB200MTTKRPValues: ptiB200MTTKRP with the tensor's values replaced by
+ * dev_vals (nnz floats in input order) -- the gradient of sum_z g_z model(z)
+ * with respect to factor `mode`.  Both run asynchronously on `stream`. */
+int ptiB200KruskalValues(ptiB200Tensor *t, const float * const *dev_factors, ptiIndex rank, ptiIndex stride,
+                         float *dev_out, void *stream);
+int ptiB200MTTKRPValues(ptiB200Tensor *t, const float *dev_vals, const void * const *dev_mats, int factor_type,
+                        ptiIndex rank, ptiIndex stride, const ptiIndex *mats_order, ptiIndex mode,
+                        float *dev_out, void *stream);
+
 /* HiCOO MTTKRP that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while it runs: code
  * whose device memory is owned by a host framework's pool, services with a
