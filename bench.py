@@ -309,6 +309,110 @@ def run_gradcp(args):
             "ms_per_gradient": round(ms, 3), "loss": float(loss.item())}
 
 
+C5_TENSORS = 256
+C5_ITERS = 20
+
+
+def make_c5(device, seed):
+    """C5: 256 3-D tensors, each mode's size U{50..5000}, nnz log-uniform in
+    [1e3, 1e6] (at most a quarter of the tensor's cells), unique uniform
+    coordinates, values U(0,1); ranks drawn from {8, 16, 32}."""
+    import torch
+    from hiparti_b200.synth import coords_torch
+    rng = np.random.default_rng(seed)
+    tensors, ranks = [], []
+    for b in range(C5_TENSORS):
+        dims = tuple(int(x) for x in rng.integers(50, 5001, 3))
+        nnz = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        nnz = min(nnz, int(np.prod(dims, dtype=np.float64)) // 4)
+        inds = coords_torch(dims, nnz, seed * 1000 + b, device=device)
+        g = torch.Generator(device=device)
+        g.manual_seed(seed * 1000 + b + 500)
+        vals = torch.rand(nnz, generator=g, device=device, dtype=torch.float32)
+        tensors.append((dims, inds, vals))
+        ranks.append(int(rng.choice([8, 16, 32])))
+    return tensors, ranks
+
+
+def run_batched(args):
+    """C5 batched uneven CPD-ALS: 256 tensors factored together, one
+    persistent launch per iteration of the whole batch replayed from a CUDA
+    graph, block size and columns per lane autotuned; FP32 and BF16 (two
+    closing FP32 sweeps) from the same U(0,1) start; fits of a sample of the
+    tensors against the FP64 oracle from the same start; the same FP32 ALS
+    run tensor by tensor through ptiB200CpdAls for comparison."""
+    import torch
+    from hiparti_b200 import DeviceTensor
+    from hiparti_b200.batched import Batch, stride_for
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tensors, ranks = make_c5(dev, SEED + 21)
+    total_nnz = sum(int(v.numel()) for _, _, v in tensors)
+    bt = Batch(tensors, ranks, tune=True)
+    info = bt.info()
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 22)
+    init = []
+    for (dims, _, _), R in zip(tensors, ranks):
+        fs = []
+        for d in dims:
+            a = torch.rand((d, stride_for(R)), generator=g, device=dev, dtype=torch.float32)
+            a[:, R:] = 0
+            fs.append(a)
+        init.append(fs)
+    out = {"workload": f"C5 batched CPD-ALS: {C5_TENSORS} 3-D tensors, dims U{{50..5000}}, nnz log-U[1e3,1e6] "
+                       f"(total {total_nnz}), U(0,1) values, ranks from {{8,16,32}}, {C5_ITERS} iterations",
+           "total_nnz": total_nnz, "sb_bits": info["sb_bits"], "cols_per_lane_bf16": info["cols_per_lane"],
+           "tasks_per_iter": info["ntasks"], "tune_s": round(info["tune_ms"] / 1e3, 3),
+           "setup_s": round(info["setup_ms"] / 1e3, 3)}
+    fits = {}
+    for prec in ["fp32", "bf16"]:
+        facs = [[a.clone() for a in fs] for fs in init]
+        bt.cpd_als(facs, 2, precision=prec, fp32_sweeps=1)  # warm-up
+        facs = [[a.clone() for a in fs] for fs in init]
+        _, f, ms = bt.cpd_als(facs, C5_ITERS, precision=prec, fp32_sweeps=2 if prec == "bf16" else C5_ITERS)
+        fits[prec] = f[:, -1]
+        out[f"ms_per_iter_{prec}"] = round(ms, 4)
+        # MTTKRP work of one iteration: every nonzero of every tensor, 3 modes
+        out[f"gnnz_modes_per_s_{prec}"] = round(3 * total_nnz / (ms * 1e-3) / 1e9, 2)
+    out["speedup_bf16_vs_fp32"] = round(out["ms_per_iter_fp32"] / out["ms_per_iter_bf16"], 3)
+    bt.free()
+    if args.batched_sequential:
+        # the same FP32 ALS, one ptiB200CpdAls call (HiCOO, sb 7) per tensor
+        dts = [DeviceTensor.from_torch_coo(d, i, v).to_hicoo(7, 7, 7) for d, i, v in tensors]
+        for t in dts:
+            t.prepare()
+        facs = [[a.clone() for a in fs] for fs in init]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for t, fs, R in zip(dts, facs, ranks):
+            t.cpd_als(fs, C5_ITERS, rank=R)
+        torch.cuda.synchronize()
+        out["ms_per_iter_fp32_tensor_by_tensor"] = round((time.perf_counter() - t0) * 1e3 / C5_ITERS, 3)
+        for t in dts:
+            t.free()
+    if args.batched_oracle > 0:
+        from oracle.oracle import Orc, ensure_built
+        ensure_built(ref=False)
+        orc = Orc()
+        order = np.argsort([int(v.numel()) for _, _, v in tensors])
+        pick = order[np.linspace(0, len(order) - 1, min(args.batched_oracle, len(order))).round().astype(int)]
+        t0 = time.perf_counter()
+        d32, d16 = [], []
+        for b in pick:
+            dims, inds, vals = tensors[b]
+            R = ranks[b]
+            o = orc.cpd_als(list(dims), [i.cpu().numpy().astype(np.uint32) for i in inds], vals.cpu().numpy(), R,
+                            C5_ITERS, [a[:, :R].cpu().numpy() for a in init[b]])
+            d32.append(abs(fits["fp32"][b] - o["fit"]))
+            d16.append(abs(fits["bf16"][b] - o["fit"]))
+        out["oracle_tensors"] = int(len(pick))
+        out["oracle_s"] = round(time.perf_counter() - t0, 1)
+        out["max_fit_diff_fp32"] = float(max(d32))
+        out["max_fit_diff_bf16"] = float(max(d16))
+    out["fit_bf16_min_max"] = [float(fits["bf16"].min()), float(fits["bf16"].max())]
+    return out
+
+
 def run_ours_mttkrp(args, rank, world):
     import torch
     from hiparti_b200 import HiCOOTensor, ffi, lib
@@ -539,6 +643,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpd", action="store_true", help="skip the CPD-ALS (C3) block")
     ap.add_argument("--no-gradcp", action="store_true", help="skip the gradient-CP (C4) block")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched CPD-ALS (C5) block")
+    ap.add_argument("--batched-oracle", type=int, default=16,
+                    help="C5 tensors (spread over the size range) checked against the FP64 oracle")
+    ap.add_argument("--batched-sequential", type=int, default=1,
+                    help="also time the C5 ALS tensor by tensor through ptiB200CpdAls")
     ap.add_argument("--cpd-iters", type=int, default=C3_ITERS)
     ap.add_argument("--cpd-format", default="hicoo", choices=["hicoo", "coo"])
     ap.add_argument("--fp32-sweeps", type=int, default=2)
@@ -570,6 +679,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["gradcp"] = run_gradcp(args)
+        if world == 1 and not args.no_batched:
+            import torch
+            torch.cuda.empty_cache()
+            res["batched"] = run_batched(args)
         print(json.dumps(res), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -29,7 +29,7 @@
 namespace pti {
 
 constexpr int kTile = 2048;        // nonzeros per CTA (COO kernel)
-constexpr int kHiTile = 2048;      // nonzeros per CTA (HiCOO kernel)
+constexpr int kHiTile = kPlanTile; // nonzeros per CTA (HiCOO kernel)
 constexpr int kHist = 2048;        // counting-sort buckets: (2048 >> sb) block rows per pass
 constexpr int kSchedThreads = 256;
 constexpr int kUnroll = 4;         // nonzeros in flight per thread group

@@ -9,6 +9,9 @@ namespace pti {
 
 constexpr int kMaxModes = 8;
 
+// Nonzeros per tile of a per-mode HiCOO schedule (HicooModePlan::tile_block).
+constexpr int kPlanTile = 2048;
+
 // Per-mode schedule of a HiCOO tensor: the blocks re-ordered by their block
 // coordinate in the output mode (a materialised form of the reference's
 // per-mode kernel scheduler kschr, src/sptensor/hicoo/convert.c:378-421), with

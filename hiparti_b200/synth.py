@@ -95,6 +95,37 @@ def planted_tensor(dims, nnz, rank, noise, seed=0):
     return inds, vals, (lam, facs)
 
 
+def sparse_lowrank_tensor(dims, rank, support, noise=0.0, seed=0):
+    """A sparse tensor of exact CP rank `rank` (plus N(0, noise^2) on its
+    nonzeros).  Component r has entries |N(0,1)| + 0.1 on `support` random rows
+    of every mode and zeros elsewhere, with weight U(1,10); the nonzeros are
+    the union of the components' support blocks, so about rank * support^N of
+    them.  Unlike values of a dense model sampled at random coordinates (which
+    leave the unsampled cells zero and make the sparse tensor high-rank), this
+    tensor is low-rank, so CPD-ALS converges to a fit near 1.
+    Returns (inds, vals, (lambda, factors))."""
+    rng = np.random.default_rng(seed)
+    facs = [np.zeros((d, rank)) for d in dims]
+    cells = []
+    for r in range(rank):
+        rows = []
+        for m, d in enumerate(dims):
+            s = min(support, d)
+            idx = rng.choice(d, s, replace=False)
+            facs[m][idx, r] = np.abs(rng.standard_normal(s)) + 0.1
+            rows.append(idx)
+        grid = np.meshgrid(*rows, indexing="ij")
+        cells.append(np.stack([g.ravel() for g in grid], 1))
+    coords = np.unique(np.concatenate(cells), axis=0)
+    inds = [coords[:, m].astype(np.uint32) for m in range(len(dims))]
+    lam = rng.uniform(1, 10, rank)
+    model = np.tile(lam, (coords.shape[0], 1))
+    for a, ix in zip(facs, inds):
+        model *= a[ix]
+    vals = (model.sum(1) + noise * rng.standard_normal(coords.shape[0])).astype(np.float32)
+    return inds, vals, (lam, facs)
+
+
 def factor_matrices(dims, R, seed=0, dist="uniform"):
     """Row-major factors with the reference's stride (R rounded up to 8); pad
     columns are zero."""

@@ -329,6 +329,39 @@ int ptiB200CpdAls(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, 
                   ptiIndex fp32_sweeps, float * const *dev_factors, ptiIndex stride, float *dev_lambda,
                   double *fits, ptiIndex *iters_done, void *stream);
 
+/* Batched CPD-ALS of many independent 3-D tensors of uneven size and rank (no
+ * counterpart in the reference, whose CPD entry points factor one tensor per
+ * call; each tensor follows src/sptensor/cpd.c:32-208).
+ *
+ * ptiB200BatchCreate copies the tensors (ndims: ntensors x 3; dev_inds:
+ * ntensors x 3 device arrays of nnz[b] uint32; dev_vals: ntensors device
+ * arrays), converts each to HiCOO on the GPU and builds its per-mode
+ * schedules.  ranks[b] in [1, 32]; every tensor needs at least one nonzero.
+ * tune != 0 times whole iterations for HiCOO block sizes sb_bits in {4..7} and
+ * 4 or 8 factor columns per lane in BF16 iterations and keeps the fastest
+ * (cached per batch shape); tune == 0 uses sb_bits 7 and 4 columns per lane.
+ *
+ * ptiB200BatchCpdAls runs niters ALS iterations on every tensor: each
+ * iteration of the whole batch is one persistent kernel launch replayed from a
+ * CUDA graph.  dev_factors: ntensors x 3 device arrays, ndims x stride FP32
+ * with stride = rank rounded up to a multiple of 8, 16-byte aligned; they hold
+ * the initial factors and receive the result.  dev_lambda: ntensors device
+ * arrays of rank floats.  precision as for ptiB200CpdAls.  fits (host,
+ * ntensors x niters, may be NULL) receives every tensor's fit after every
+ * iteration; ms_per_iter (may be NULL) the device time of one iteration of the
+ * batch.  Synchronous; ordered after the work already queued on `stream`. */
+typedef struct ptiB200Batch ptiB200Batch;
+int ptiB200BatchCreate(ptiB200Batch **out, ptiIndex ntensors, const ptiIndex *ndims,
+                       const ptiNnzIndex *nnz, const ptiIndex * const *dev_inds,
+                       const ptiValue * const *dev_vals, const ptiIndex *ranks, int tune,
+                       void *stream);
+int ptiB200BatchInfo(const ptiB200Batch *batch, int *sb_bits, int *cols_per_lane, float *tune_ms,
+                     float *setup_ms, ptiNnzIndex *ntasks);
+int ptiB200BatchCpdAls(ptiB200Batch *batch, ptiIndex niters, int precision, ptiIndex fp32_sweeps,
+                       float * const *dev_factors, float * const *dev_lambda, double *fits,
+                       float *ms_per_iter, void *stream);
+void ptiB200BatchFree(ptiB200Batch *batch);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

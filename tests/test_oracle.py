@@ -109,3 +109,12 @@ def test_orc_cpd_vs_reference_library(orc, ref):
     for m in range(4):
         assert rel_err(o["factors"][m], facs[m]) < 1e-4
     assert rel_err(o["lambda_"], lam) < 1e-4
+
+
+def test_sparse_lowrank_generator_is_exactly_low_rank(orc):
+    # the generating model reproduces every nonzero: fit 1 with no noise
+    dims = (40, 30, 20)
+    inds, vals, (lam, facs) = synth.sparse_lowrank_tensor(dims, 4, 5, 0.0, seed=3)
+    assert vals.size > 200 and np.all(vals > 0)
+    fit = orc.kruskal_fit(dims, inds, vals, lam, facs)
+    assert abs(fit - 1.0) < 1e-6
