@@ -8,9 +8,9 @@
 // launch of a persistent kernel whose CTAs pull tasks from a queue:
 //
 //   tile task  (b, m, t)  MTTKRP of tile t of tensor b's mode-m schedule into
-//                         M_bm (the sched.cu tile algorithm: bulk-copied tile,
-//                         in-CTA counting sort by output row, one vector atomic
-//                         per row run and thread group)
+//                         M_bm (as in sched.cu: bulk-copied tile already in
+//                         output-row order, one vector atomic per row run and
+//                         thread group)
 //   dense task (b, m)     the mode-m ALS step of tensor b, in FP64:
 //                         W = (G_a o G_b)^-1 (Cholesky; Gauss-Jordan fallback),
 //                         A_bm = M_bm W, lambda (2-norm in iteration 0, else
@@ -55,7 +55,6 @@ namespace pti {
 constexpr int kBThreads = 256;
 constexpr int kBMaxRank = 32;
 constexpr int kBTile = kPlanTile;
-constexpr int kBHist = 2048;                    // counting-sort buckets: (2048 >> sb) block rows per pass
 constexpr uint64_t kWaitNs = 2000000000ull;     // bound of every dependency wait: 2 s
 
 // error bits of the batch's error word
@@ -63,7 +62,7 @@ constexpr uint32_t kErrRange = 1u, kErrCopy = 2u, kErrWait = 4u;
 
 struct BatchPlan {        // the mode-m schedule of tensor b
     uint64_t nnz, nb;
-    const uint64_t *bptr;
+    const uint16_t *lblk;             // block of each nonzero within its tile
     const uint32_t *tile_block;
     const uint32_t *out_bind;
     const uint32_t *in_bind[2];
@@ -169,9 +168,7 @@ struct TileSmem {
     static constexpr uint32_t eout = val + 4 * kBTile;          // u8[kBTile]
     static constexpr uint32_t ein = eout + kBTile;              // u8[2][kBTile]
     static constexpr uint32_t blk = ein + 2 * kBTile;           // u16[kBTile]
-    static constexpr uint32_t ord = blk + 2 * kBTile;           // u16[kBTile]
-    static constexpr uint32_t hist = ord + 2 * kBTile;          // u32[kBHist]
-    static constexpr uint32_t brow = hist + 4 * kBHist;         // u32[kBTile + 4]
+    static constexpr uint32_t brow = blk + 2 * kBTile;          // u32[kBTile + 4]
     static constexpr uint32_t bin = brow + 4 * (kBTile + 4);    // u32[2][kBTile + 4]
     static constexpr uint32_t total = bin + 8 * (kBTile + 4);
 };
@@ -193,18 +190,18 @@ __device__ __forceinline__ uint32_t round16u(uint32_t x) { return (x + 15u) & ~1
 
 // One tile of a mode-m schedule: a group of 2^glog lanes x CPL columns per
 // nonzero (the group size is chosen from the tensor's rank at run time, so a
-// kernel holds one tile variant).
+// kernel holds one tile variant).  The schedule keeps each tile's nonzeros in
+// output-row order, so a group walks a contiguous slice and adds a row into
+// M once per run.
 template <int CPL, class FT>
 __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsigned char *sm, uint64_t *mbar,
-                          uint32_t &phase, uint32_t *s_scan, uint32_t *err)
+                          uint32_t &phase, uint32_t *err)
 {
     constexpr int U = 4;  // nonzeros in flight per group
     float *s_val = reinterpret_cast<float *>(sm + TileSmem::val);
     uint8_t *s_eout = sm + TileSmem::eout;
     uint8_t *s_ein = sm + TileSmem::ein;
     uint16_t *s_blk = reinterpret_cast<uint16_t *>(sm + TileSmem::blk);
-    uint16_t *s_ord = reinterpret_cast<uint16_t *>(sm + TileSmem::ord);
-    uint32_t *s_hist = reinterpret_cast<uint32_t *>(sm + TileSmem::hist);
     uint32_t *s_brow = reinterpret_cast<uint32_t *>(sm + TileSmem::brow);
     uint32_t *s_bin = reinterpret_cast<uint32_t *>(sm + TileSmem::bin);
     const uint32_t tid = threadIdx.x;
@@ -218,27 +215,20 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
     uint32_t nblk = __ldg(gp->tile_block + tile + 1) - b0 + 1;
     if (nblk > kBTile + 1) nblk = kBTile + 1;
     if (b0 + (uint64_t)nblk > nb) nblk = (uint32_t)(nb - b0);
+    const uint32_t bo4 = b0 & 3u;  // block coordinates are copied from b0 rounded down to 16 bytes
 
     if (tid == 0) {
-        const uint32_t be = round16u(n), bv = round16u(4 * n);
-        mbar_arrive_expect_tx(mbar, bv + 3 * be);
+        const uint32_t be = round16u(n), bv = round16u(4 * n), bl = round16u(2 * n);
+        const uint32_t bb = 4 * ((nblk + bo4 + 3) & ~3u);
+        mbar_arrive_expect_tx(mbar, bv + 3 * be + bl + 3 * bb);
         bulk_g2s(s_val, gp->vals + z0, bv, mbar);
         bulk_g2s(s_eout, gp->out_eind + z0, be, mbar);
         bulk_g2s(s_ein, gp->in_eind[0] + z0, be, mbar);
         bulk_g2s(s_ein + kBTile, gp->in_eind[1] + z0, be, mbar);
-    }
-    {
-        const uint64_t *bptr = gp->bptr;
-        const uint32_t *ob = gp->out_bind, *ib0 = gp->in_bind[0], *ib1 = gp->in_bind[1];
-        for (uint32_t i = tid; i < nblk; i += kBThreads) {
-            const uint64_t b = b0 + i;
-            s_brow[i] = __ldg(ob + b);
-            s_bin[i] = __ldg(ib0 + b) << sb;
-            s_bin[(kBTile + 4) + i] = __ldg(ib1 + b) << sb;
-            const uint64_t lo = __ldg(bptr + b), hi = __ldg(bptr + b + 1);
-            const uint64_t zs = lo > z0 ? lo : z0, ze = hi < z0 + n ? hi : z0 + n;
-            for (uint64_t z = zs; z < ze; ++z) s_blk[z - z0] = (uint16_t)i;
-        }
+        bulk_g2s(s_blk, gp->lblk + z0, bl, mbar);
+        bulk_g2s(s_brow, gp->out_bind + (b0 - bo4), bb, mbar);
+        bulk_g2s(s_bin, gp->in_bind[0] + (b0 - bo4), bb, mbar);
+        bulk_g2s(s_bin + (kBTile + 4), gp->in_bind[1] + (b0 - bo4), bb, mbar);
     }
     const bool ok = mbar_wait_bounded(mbar, phase);
     phase ^= 1u;
@@ -246,6 +236,8 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
         if (tid == 0) atomicOr(err, kErrCopy);
         return;
     }
+    s_brow += bo4;
+    s_bin += bo4;
 
     const FT *mat0, *mat1;
     if constexpr (sizeof(FT) == 4) {
@@ -262,112 +254,60 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
     const uint32_t kGroups = (uint32_t)kBThreads >> glog;
     const uint32_t col = lane * CPL;
     const bool active = col < R;
-    const uint32_t span = (uint32_t)kBHist >> sb;
-    uint32_t zs = 0;
-    while (zs < n) {
-        // this pass: nonzeros whose block row is < br0 + span
-        const uint32_t br0 = s_brow[s_blk[zs]];
-        uint32_t lo = zs + 1, hi = n;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_brow[s_blk[mid]] - br0 >= span) hi = mid;
-            else lo = mid + 1;
-        }
-        const uint32_t ze = lo;
-        for (uint32_t h = tid; h < (uint32_t)kBHist; h += kBThreads) s_hist[h] = 0;
-        __syncthreads();
-        for (uint32_t z = zs + tid; z < ze; z += kBThreads)
-            atomicAdd(&s_hist[((s_brow[s_blk[z]] - br0) << sb) | s_eout[z]], 1u);
-        __syncthreads();
-        {   // exclusive scan of the histogram
-            constexpr int per = kBHist / kBThreads;
-            uint32_t v[per], sum = 0;
+    // an odd slice length puts the groups' first nonzeros on different banks
+    const uint32_t per = ((n + kGroups - 1) >> (8u - glog)) | 1u;
+    const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
+    float acc[CPL];
 #pragma unroll
-            for (int j = 0; j < per; ++j) {
-                v[j] = s_hist[tid * per + j];
-                sum += v[j];
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+    uint32_t cur = 0xFFFFFFFFu;
+    auto flush = [&](uint32_t row) {
+#pragma unroll
+        for (int q = 0; q < CPL / 4; ++q)
+            if (col + 4 * q < R)
+                red_add4(out + (size_t)row * stride + col + 4 * q,
+                         mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]),
+                               col + 4 * q, R));
+    };
+    for (uint32_t j = j0; j < j1; j += U) {
+        uint32_t orow[U];
+        float v[U];
+        Cols<CPL, FT> f0[U], f1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            orow[u] = 0xFFFFFFFFu;
+            if (j + u >= j1) continue;
+            const uint32_t z = j + u, i = s_blk[z];
+            const uint32_t o = (s_brow[i] << sb) + s_eout[z];
+            const uint32_t r0 = (s_bin[i] << sb) + s_ein[z];
+            const uint32_t r1 = (s_bin[(kBTile + 4) + i] << sb) + s_ein[kBTile + z];
+            v[u] = s_val[z];
+            if (!(i < nblk && o < out_dim && r0 < in_dim0 && r1 < in_dim1)) {
+                if (lane == 0) atomicOr(err, kErrRange);
+                continue;
             }
-            uint32_t x = sum;
-            const uint32_t l = tid & 31, w = tid >> 5;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if (l >= (uint32_t)o) x += y;
-            }
-            if (l == 31) s_scan[w] = x;
-            __syncthreads();
-            uint32_t wp = 0;
-            for (uint32_t q = 0; q < w; ++q) wp += s_scan[q];
-            uint32_t run = wp + x - sum + zs;
-#pragma unroll
-            for (int j = 0; j < per; ++j) {
-                s_hist[tid * per + j] = run;
-                run += v[j];
+            orow[u] = o;
+            if (active) {
+                f0[u].load(mat0 + (size_t)r0 * stride, col);
+                f1[u].load(mat1 + (size_t)r1 * stride, col);
             }
         }
-        __syncthreads();
-        for (uint32_t z = zs + tid; z < ze; z += kBThreads) {
-            const uint32_t pos = atomicAdd(&s_hist[((s_brow[s_blk[z]] - br0) << sb) | s_eout[z]], 1u);
-            s_ord[pos] = (uint16_t)z;
-        }
-        __syncthreads();
-
-        const uint32_t cnt = ze - zs, per = ((cnt + kGroups - 1) >> (8u - glog)) | 1u;
-        const uint32_t j0 = min(zs + g * per, ze), j1 = min(j0 + per, ze);
-        float acc[CPL];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-        uint32_t cur = 0xFFFFFFFFu;
-        auto flush = [&](uint32_t row) {
+        for (int u = 0; u < U; ++u) {
+            if (orow[u] == 0xFFFFFFFFu) continue;
+            if (orow[u] != cur) {
+                if (cur != 0xFFFFFFFFu && active) flush(cur);
 #pragma unroll
-            for (int q = 0; q < CPL / 4; ++q)
-                if (col + 4 * q < R)
-                    red_add4(out + (size_t)row * stride + col + 4 * q,
-                             mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]),
-                                   col + 4 * q, R));
-        };
-        for (uint32_t j = j0; j < j1; j += U) {
-            uint32_t orow[U];
-            float v[U];
-            Cols<CPL, FT> f0[U], f1[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                orow[u] = 0xFFFFFFFFu;
-                if (j + u >= j1) continue;
-                const uint32_t z = s_ord[j + u], i = s_blk[z];
-                const uint32_t o = (s_brow[i] << sb) + s_eout[z];
-                const uint32_t r0 = s_bin[i] + s_ein[z];
-                const uint32_t r1 = s_bin[(kBTile + 4) + i] + s_ein[kBTile + z];
-                v[u] = s_val[z];
-                if (!(o < out_dim && r0 < in_dim0 && r1 < in_dim1)) {
-                    if (lane == 0) atomicOr(err, kErrRange);
-                    continue;
-                }
-                orow[u] = o;
-                if (active) {
-                    f0[u].load(mat0 + (size_t)r0 * stride, col);
-                    f1[u].load(mat1 + (size_t)r1 * stride, col);
-                }
+                for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+                cur = orow[u];
             }
+            if (active) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (orow[u] == 0xFFFFFFFFu) continue;
-                if (orow[u] != cur) {
-                    if (cur != 0xFFFFFFFFu && active) flush(cur);
-#pragma unroll
-                    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-                    cur = orow[u];
-                }
-                if (active) {
-#pragma unroll
-                    for (int c = 0; c < CPL; ++c) acc[c] += v[u] * f0[u].at(c) * f1[u].at(c);
-                }
+                for (int c = 0; c < CPL; ++c) acc[c] += v[u] * f0[u].at(c) * f1[u].at(c);
             }
         }
-        if (cur != 0xFFFFFFFFu && active) flush(cur);
-        __syncthreads();
-        zs = ze;
     }
+    if (cur != 0xFFFFFFFFu && active) flush(cur);
 }
 
 // W = V^-1 for a symmetric R x R matrix (R <= 32) in FP64 shared memory, by
@@ -635,7 +575,6 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ uint64_t mbar;
-    __shared__ uint32_t s_scan[kBThreads / 32];
     __shared__ uint32_t s_q;
     __shared__ int s_ok;
     const uint32_t tid = threadIdx.x;
@@ -665,7 +604,7 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
         __syncthreads();
         if (s_ok) {
             if (dense) dense_task(a.tens + b, b, m, it, a, sm);
-            else tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, s_scan, a.err);
+            else tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err);
         }
         // shared memory written by this task may next be filled by bulk copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -833,7 +772,7 @@ int batch_build_plans(ptiB200Batch *bt, int sb)
             BatchPlan p{};
             p.nnz = h->nnz;
             p.nb = P.nb;
-            p.bptr = P.bptr.as<uint64_t>();
+            p.lblk = P.lblk.as<uint16_t>();
             p.tile_block = P.tile_block.as<uint32_t>();
             p.out_bind = P.binds[m].as<uint32_t>();
             p.out_eind = P.einds[m].as<uint8_t>();

@@ -6,21 +6,21 @@
 //
 // Schedule (built once per tensor and mode, kept in the device handle).
 // HiCOO: the blocks are stably re-ordered by their block coordinate in the
-// output mode, and the nonzeros of each block by their 8-bit output offset --
-// the reference's per-mode kernel scheduler (kschr, src/sptensor/hicoo/
-// convert.c:378-421) taken down to block granularity and materialised as a
-// second HiCOO array set.  COO: the nonzeros are stably sorted by their
-// output index.
+// output mode -- the reference's per-mode kernel scheduler (kschr,
+// src/sptensor/hicoo/convert.c:378-421) taken down to block granularity --
+// and the nonzeros follow their blocks; the nonzeros are then cut into tiles
+// of kPlanTile and re-ordered by output row inside each tile, each keeping its
+// 8-bit element offsets and the index of its block among the tile's blocks.
+// COO: the nonzeros are stably sorted by their output index and packed as
+// records {output index, operand indices, value}.
 //
-// Kernel (one CTA per tile of kTile nonzeros).  The tile's element offsets and
-// values are staged into shared memory with bulk (TMA) copies; block
-// coordinates are loaded alongside and every nonzero is tagged with its block.
-// For HiCOO the tile is then counting-sorted by output row in shared memory
-// (at most 1024 >> sb block rows at a time), so each thread group walks a
-// contiguous run of nonzeros ordered by output row, accumulates the rank-R
-// Hadamard products in registers and adds a row into global memory once per
-// run (16-byte vector atomics).  A hot row is thus added once per group that
-// touches it instead of once per nonzero.
+// Kernels (one CTA per tile).  The tile is staged into shared memory with
+// bulk (TMA) copies.  Its nonzeros are in output-row order, so each thread
+// group walks a contiguous slice, gathers the operand rows with 16-byte
+// loads, accumulates the rank-R Hadamard products in registers and adds a row
+// into global memory once per run of equal rows (16-byte vector atomics); a
+// row shared by neighbouring groups is merged in shared memory first, so a hot
+// row costs one global add per tile instead of one per nonzero.
 #include "kutil.cuh"
 #include "primitives.cuh"
 #include "tensor.cuh"
@@ -30,9 +30,7 @@ namespace pti {
 
 constexpr int kTile = 2048;        // nonzeros per CTA (COO kernel)
 constexpr int kHiTile = kPlanTile; // nonzeros per CTA (HiCOO kernel)
-constexpr int kHist = 2048;        // counting-sort buckets: (2048 >> sb) block rows per pass
 constexpr int kSchedThreads = 256;
-constexpr int kUnroll = 4;         // nonzeros in flight per thread group
 
 uint32_t *err_word();
 int ensure_err_word(cudaStream_t s);
@@ -40,7 +38,7 @@ int ensure_err_word(cudaStream_t s);
 struct SchedArgs {
     uint64_t nnz, nb;
     uint32_t R, stride, sb;
-    const uint64_t *bptr;
+    const uint16_t *lblk;       // HiCOO: block of each nonzero within its tile
     const uint32_t *tile_block;
     const uint32_t *out_bind;   // HiCOO: block coords of the output mode; COO: output indices
     const uint8_t *out_eind;
@@ -93,103 +91,194 @@ struct RowPart {
     }
 };
 
-// Walks records [j0, j1) (ordered by output row): gathers the operand rows,
-// accumulates v * prod_k A_k[row_k] in registers, and adds the sum into the
-// output once per run of equal output rows.
-template <int G, int CPL, int U, int NIN, class FT>
-__device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t j0, uint32_t j1, uint32_t lane,
-                                                const SchedArgs &a, const float *alt = nullptr)
-{
-    constexpr int RW = Rec<NIN>::words;
-    const uint32_t col = lane * CPL;
-    const bool active = col < a.R;
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+
+// Row runs of one thread group.  Products arrive in output-row order; a run
+// that ends is added into the output with one vector atomic per 4 columns,
+// except the runs a group shares with its neighbours in the CTA: the run that
+// continues the previous group's last row is parked in the group's merge slot
+// (shared memory), and the run that continues into the next group stays in
+// registers until merge(), where the group that started the row adds the
+// parked parts and writes the row once.  A row that fills many slices of a
+// tile (a hot row of a power-law mode) is so written once per tile instead of
+// once per group.
+template <int CPL>
+struct RunWriter {
     float acc[CPL];
+    uint32_t cur = kNoRow;
+    bool in_first = true, first_shared, last_shared, active;
+    uint32_t col;
+    float *slot;  // this lane's CPL floats of the group's merge slot
+
+    __device__ __forceinline__ RunWriter(bool fs, bool ls, uint32_t col_, bool active_, float *slot_)
+        : first_shared(fs), last_shared(ls), active(active_), col(col_), slot(slot_)
+    {
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-    uint32_t cur = 0xFFFFFFFFu;
-    auto flush = [&](uint32_t row) {
+        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+    }
+    __device__ __forceinline__ void flush(const SchedArgs &a)
+    {
+        if (!active) return;
 #pragma unroll
         for (int q = 0; q < CPL / 4; ++q)
             if (col + 4 * q < a.R)
-                red_add4(a.out + (size_t)row * a.stride + col + 4 * q,
-                         mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]), col + 4 * q, a.R));
-    };
+                red_add4(a.out + (size_t)cur * a.stride + col + 4 * q,
+                         mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]),
+                               col + 4 * q, a.R));
+    }
+    __device__ __forceinline__ void park()
+    {
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) slot[c] = acc[c];
+    }
+    // a product for `row` follows
+    __device__ __forceinline__ void start(uint32_t row, const SchedArgs &a)
+    {
+        if (row == cur) return;
+        if (cur != kNoRow) {
+            if (in_first && first_shared) park();
+            else flush(a);
+            in_first = false;
+        }
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+        cur = row;
+    }
+    // after the slice: true if this group owns a row that continues into the
+    // next group (merge() after a barrier)
+    __device__ __forceinline__ bool finish(const SchedArgs &a)
+    {
+        if (cur == kNoRow) return false;
+        if (in_first && first_shared) {
+            park();
+            return false;
+        }
+        if (last_shared) return true;
+        flush(a);
+        return false;
+    }
+    // adds the parked parts of the following groups that continue row `cur`
+    // and writes the row
+    template <int G>
+    __device__ __forceinline__ void merge(const SchedArgs &a, const float *slots, const uint32_t *slot_row,
+                                          const uint8_t *slot_whole, uint32_t g, uint32_t lane, uint32_t ngroups)
+    {
+        for (uint32_t h = g + 1; h < ngroups; ++h) {
+            if (slot_row[h] != cur) break;
+            const float *p = slots + ((size_t)h * G + lane) * CPL;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) acc[c] += p[c];
+            if (!slot_whole[h]) break;
+        }
+        flush(a);
+    }
+};
+
+// Walks records [j0, j1) (ordered by output row) of a tile whose records are
+// s_rec[0, n): gathers the operand rows and accumulates v * prod_k A_k[row_k]
+// in registers, one output row run at a time (RunWriter).
+template <int G, int CPL, int U, int NIN, class FT>
+__device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t n, uint32_t j0, uint32_t j1,
+                                                uint32_t g, uint32_t lane, const SchedArgs &a, const float *alt,
+                                                float *s_slots, uint32_t *s_slot_row, uint8_t *s_slot_whole)
+{
+    constexpr int RW = Rec<NIN>::words;
+    constexpr uint32_t kGroups = kSchedThreads / G;
+    const uint32_t col = lane * CPL;
+    const bool active = col < a.R;
+    bool first_shared = false, last_shared = false;
+    if (j0 < j1) {
+        const uint32_t rf = s_rec[(size_t)j0 * RW], rl = s_rec[(size_t)(j1 - 1) * RW];
+        first_shared = j0 > 0 && s_rec[(size_t)(j0 - 1) * RW] == rf;
+        last_shared = j1 < n && s_rec[(size_t)j1 * RW] == rl;
+        if (lane == 0) {
+            s_slot_row[g] = first_shared ? rf : kNoRow;
+            s_slot_whole[g] = rf == rl;
+        }
+    } else if (lane == 0) {
+        s_slot_row[g] = kNoRow;
+        s_slot_whole[g] = 0;
+    }
+    RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
     for (uint32_t j = j0; j < j1; j += U) {
         uint32_t orow[U];
         float val[U];
         RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            orow[u] = 0xFFFFFFFFu;
+            orow[u] = kNoRow;
             if (j + u < j1) {
-                uint32_t w[RW];
+                uint32_t wd[RW];
 #pragma unroll
                 for (int q = 0; q < RW; q += 4) {
                     const uint4 r = *reinterpret_cast<const uint4 *>(s_rec + (size_t)(j + u) * RW + q);
-                    w[q] = r.x; w[q + 1] = r.y; w[q + 2] = r.z; w[q + 3] = r.w;
+                    wd[q] = r.x; wd[q + 1] = r.y; wd[q + 2] = r.z; wd[q + 3] = r.w;
                 }
-                orow[u] = w[0];
-                val[u] = alt ? __ldg(alt + j + u) : __uint_as_float(w[1 + NIN]);
-                if (orow[u] != 0xFFFFFFFFu && active) {
+                orow[u] = wd[0];
+                val[u] = alt ? __ldg(alt + j + u) : __uint_as_float(wd[1 + NIN]);
+                if (orow[u] != kNoRow && active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
-                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)w[1 + k] * a.stride, col);
+                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)wd[1 + k] * a.stride, col);
                 }
             }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (orow[u] == 0xFFFFFFFFu) continue;
-            if (orow[u] != cur) {
-                if (cur != 0xFFFFFFFFu && active) flush(cur);
-#pragma unroll
-                for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-                cur = orow[u];
-            }
+            if (orow[u] == kNoRow) continue;
+            w.start(orow[u], a);
             if (active) {
 #pragma unroll
                 for (int c = 0; c < CPL; ++c) {
                     float p = val[u] * f[u][0].at(c);
 #pragma unroll
                     for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
-                    acc[c] += p;
+                    w.acc[c] += p;
                 }
             }
         }
     }
-    if (cur != 0xFFFFFFFFu && active) flush(cur);
+    const bool owner = w.finish(a);
+    __syncthreads();
+    if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
 }
 
-template <int NIN>
+template <int NIN, int CPL>
 struct HiSmem {
     // byte offsets inside the dynamic shared memory of hicoo_sched_kernel
     static constexpr uint32_t val = 0;                                  // float[kHiTile]
     static constexpr uint32_t eout = val + 4 * kHiTile;                 // u8[kHiTile]
     static constexpr uint32_t ein = eout + kHiTile;                     // u8[NIN][kHiTile]
     static constexpr uint32_t blk = ein + NIN * kHiTile;                // u16[kHiTile]
-    static constexpr uint32_t ord = blk + 2 * kHiTile;                  // u16[kHiTile]
-    static constexpr uint32_t hist = ord + 2 * kHiTile;                 // u32[kHist]
-    static constexpr uint32_t brow = hist + 4 * kHist;                  // u32[kHiTile + 4]
+    static constexpr uint32_t brow = blk + 2 * kHiTile;                 // u32[kHiTile + 4]
     static constexpr uint32_t bin = brow + 4 * (kHiTile + 4);           // u32[NIN][kHiTile + 4]
-    static constexpr uint32_t total = bin + 4 * NIN * (kHiTile + 4);
+    static constexpr uint32_t slots = bin + 4 * NIN * (kHiTile + 4);    // float[kSchedThreads * CPL]
+    static constexpr uint32_t total = slots + 4 * kSchedThreads * CPL;
 };
 
+// HiCOO schedule, one CTA per tile of kHiTile nonzeros.  The tile's nonzeros
+// (8-bit element offsets, values, block index within the tile) and its blocks'
+// coordinates are staged into shared memory with bulk copies; the nonzeros
+// are already in output-row order (the schedule sorted each tile), so every
+// thread group walks a contiguous slice: a lane decodes one nonzero's output
+// and operand rows from its block coordinates and offsets, the group shares
+// them by shuffles, gathers the operand rows and accumulates row runs.
 template <int G, int CPL, class FT, int NIN>
 __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 {
-    using L = HiSmem<NIN>;
+    using L = HiSmem<NIN, CPL>;
     constexpr int U = NIN <= 2 ? 4 : 2;  // nonzeros in flight per group
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ uint64_t mbar;
-    __shared__ uint32_t s_scan[kSchedThreads / 32];
+    __shared__ uint32_t s_slot_row[kSchedThreads];
+    __shared__ uint8_t s_slot_whole[kSchedThreads];
     float *s_val = reinterpret_cast<float *>(sm + L::val);
     uint8_t *s_eout = sm + L::eout;
     uint8_t *s_ein = sm + L::ein;
     uint16_t *s_blk = reinterpret_cast<uint16_t *>(sm + L::blk);
-    uint16_t *s_ord = reinterpret_cast<uint16_t *>(sm + L::ord);
-    uint32_t *s_hist = reinterpret_cast<uint32_t *>(sm + L::hist);
     uint32_t *s_brow = reinterpret_cast<uint32_t *>(sm + L::brow);
     uint32_t *s_bin = reinterpret_cast<uint32_t *>(sm + L::bin);
+    float *s_slots = reinterpret_cast<float *>(sm + L::slots);
     const uint32_t tid = threadIdx.x;
 
     const uint64_t z0 = (uint64_t)blockIdx.x * kHiTile;
@@ -199,28 +288,26 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
     if (nblk > kHiTile + 1) nblk = kHiTile + 1;
     if (b0 + (uint64_t)nblk > a.nb) nblk = (uint32_t)(a.nb - b0);
 
-    // stage element offsets and values with bulk copies
+    // Stage the tile with bulk copies.  A bulk copy starts on 16 bytes, so the
+    // block coordinates are copied from b0 rounded down to 4 entries.
+    const uint32_t bo4 = b0 & 3u;
     if (tid == 0) {
         mbar_init(&mbar, 1);
         mbar_fence_init();
     }
     __syncthreads();
     if (tid == 0) {
-        const uint32_t be = round16(n), bv = round16(4 * n);
-        mbar_arrive_expect_tx(&mbar, bv + (NIN + 1) * be);
+        const uint32_t be = round16(n), bv = round16(4 * n), bl = round16(2 * n);
+        const uint32_t bb = 4 * ((nblk + bo4 + 3) & ~3u);
+        mbar_arrive_expect_tx(&mbar, bv + (NIN + 1) * be + bl + (NIN + 1) * bb);
         bulk_g2s(s_val, a.vals + z0, bv, &mbar);
         bulk_g2s(s_eout, a.out_eind + z0, be, &mbar);
 #pragma unroll
         for (int k = 0; k < NIN; ++k) bulk_g2s(s_ein + k * kHiTile, a.in_eind[k] + z0, be, &mbar);
-    }
-    // block coordinates and the block of every nonzero, meanwhile
-    for (uint32_t i = tid; i < nblk; i += kSchedThreads) {
-        const uint64_t b = b0 + i;
-        s_brow[i] = __ldg(a.out_bind + b);
+        bulk_g2s(s_blk, a.lblk + z0, bl, &mbar);
+        bulk_g2s(s_brow, a.out_bind + (b0 - bo4), bb, &mbar);
 #pragma unroll
-        for (int k = 0; k < NIN; ++k) s_bin[k * (kHiTile + 4) + i] = __ldg(a.in_bind[k] + b) << a.sb;
-        const uint64_t zs = max(__ldg(a.bptr + b), z0), ze = min(__ldg(a.bptr + b + 1), z0 + n);
-        for (uint64_t z = zs; z < ze; ++z) s_blk[z - z0] = (uint16_t)i;
+        for (int k = 0; k < NIN; ++k) bulk_g2s(s_bin + k * (kHiTile + 4), a.in_bind[k] + (b0 - bo4), bb, &mbar);
     }
     const bool ok = mbar_wait_bounded(&mbar, 0);
     if (!__syncthreads_and(ok)) {
@@ -230,100 +317,78 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         }
         return;
     }
+    s_brow += bo4;  // block i of the tile is entry i + bo4 of the staged coordinates
+    s_bin += bo4;
 
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
+    // Each step a group decodes D nonzeros of its slice, Q per lane, and hands
+    // them to its lanes by shuffles.
+    constexpr int D = G >= U ? G : U;
+    constexpr int Q = D / G;
     const uint32_t col = lane * CPL;
     const bool active = col < a.R;
-    const uint32_t span = (uint32_t)kHist >> a.sb;
-    uint32_t zs = 0;
-    while (zs < n) {
-        // the pass covers nonzeros whose block row is < br0 + span
-        const uint32_t br0 = s_brow[s_blk[zs]];
-        uint32_t lo = zs + 1, hi = n;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_brow[s_blk[mid]] - br0 >= span) hi = mid;
-            else lo = mid + 1;
+    auto row_at = [&](uint32_t z) {
+        const uint32_t i = s_blk[z];
+        return i < nblk ? (s_brow[i] << a.sb) + s_eout[z] : kNoRow;
+    };
+    // an odd slice length puts the groups' first nonzeros on different shared-memory banks
+    const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;
+    const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
+    bool first_shared = false, last_shared = false;
+    if (j0 < j1) {
+        const uint32_t rf = row_at(j0), rl = row_at(j1 - 1);
+        first_shared = j0 > 0 && row_at(j0 - 1) == rf;
+        last_shared = j1 < n && row_at(j1) == rl;
+        if (lane == 0) {
+            s_slot_row[g] = first_shared ? rf : kNoRow;
+            s_slot_whole[g] = rf == rl;
         }
-        const uint32_t ze = lo;
-        for (uint32_t h = tid; h < (uint32_t)kHist; h += kSchedThreads) s_hist[h] = 0;
-        __syncthreads();
-        for (uint32_t z = zs + tid; z < ze; z += kSchedThreads)
-            atomicAdd(&s_hist[((s_brow[s_blk[z]] - br0) << a.sb) | s_eout[z]], 1u);
-        __syncthreads();
-        {   // exclusive scan of the histogram (kHist = 256 threads x 8)
-            constexpr int per = kHist / kSchedThreads;
-            uint32_t v[per], sum = 0;
+    } else if (lane == 0) {
+        s_slot_row[g] = kNoRow;
+        s_slot_whole[g] = 0;
+    }
+    RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
+    const uint32_t nsteps = (per + D - 1) / D;  // the same for every group: shuffles stay warp-uniform
+    for (uint32_t step = 0; step < nsteps; ++step) {
+        const uint32_t jb = j0 + step * D;
+        uint32_t my_o[Q], my_r[Q][NIN];
+        float my_v[Q];
 #pragma unroll
-            for (int j = 0; j < per; ++j) {
-                v[j] = s_hist[tid * per + j];
-                sum += v[j];
-            }
-            uint32_t x = sum;
-            const uint32_t l = tid & 31, w = tid >> 5;
+        for (int q = 0; q < Q; ++q) {
+            const uint32_t z = jb + q * G + lane;
+            my_o[q] = kNoRow;
+            my_v[q] = 0.f;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if (l >= (uint32_t)o) x += y;
-            }
-            if (l == 31) s_scan[w] = x;
-            __syncthreads();
-            uint32_t wp = 0;
-            for (uint32_t q = 0; q < w; ++q) wp += s_scan[q];
-            uint32_t run = wp + x - sum + zs;
+            for (int k = 0; k < NIN; ++k) my_r[q][k] = 0;
+            if (z < j1) {
+                const uint32_t i = s_blk[z];
+                const uint32_t o = (s_brow[i] << a.sb) + s_eout[z];
+                bool ok_z = i < nblk && o < a.out_dim;
 #pragma unroll
-            for (int j = 0; j < per; ++j) {
-                s_hist[tid * per + j] = run;
-                run += v[j];
+                for (int k = 0; k < NIN; ++k) {
+                    my_r[q][k] = (s_bin[k * (kHiTile + 4) + i] << a.sb) + s_ein[k * kHiTile + z];
+                    ok_z = ok_z && my_r[q][k] < a.in_dim[k];
+                }
+                my_v[q] = s_val[z];
+                if (ok_z) my_o[q] = o;
+                else atomicOr(a.err, 1u);
             }
         }
-        __syncthreads();
-        for (uint32_t z = zs + tid; z < ze; z += kSchedThreads) {
-            const uint32_t pos = atomicAdd(&s_hist[((s_brow[s_blk[z]] - br0) << a.sb) | s_eout[z]], 1u);
-            s_ord[pos] = (uint16_t)z;
-        }
-        __syncthreads();
-
-        // each group: a contiguous run of the row-sorted nonzeros
-        // an odd slice length puts the groups' first records on different shared-memory banks
-        const uint32_t cnt = ze - zs, per = ((cnt + kGroups - 1) / kGroups) | 1u;
-        const uint32_t j0 = min(zs + g * per, ze), j1 = min(j0 + per, ze);
-        float acc[CPL];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-        uint32_t cur = 0xFFFFFFFFu;
-        auto flush = [&](uint32_t row) {
-#pragma unroll
-            for (int q = 0; q < CPL / 4; ++q)
-                if (col + 4 * q < a.R)
-                    red_add4(a.out + (size_t)row * a.stride + col + 4 * q,
-                             mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]), col + 4 * q, a.R));
-        };
-        for (uint32_t j = j0; j < j1; j += U) {
+        for (int t0 = 0; t0 < D; t0 += U) {
             uint32_t orow[U];
             float v[U];
             RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                orow[u] = 0xFFFFFFFFu;
-                if (j + u >= j1) continue;
-                const uint32_t z = s_ord[j + u], i = s_blk[z];
-                const uint32_t o = (s_brow[i] << a.sb) + s_eout[z];
-                v[u] = s_val[z];
-                bool in_range = o < a.out_dim;
+                const int t = t0 + u, src = t % G, q = t / G;
+                orow[u] = __shfl_sync(0xffffffffu, my_o[q], src, G);
+                v[u] = __shfl_sync(0xffffffffu, my_v[q], src, G);
                 uint32_t r[NIN];
 #pragma unroll
-                for (int k = 0; k < NIN; ++k) {
-                    r[k] = s_bin[k * (kHiTile + 4) + i] + s_ein[k * kHiTile + z];
-                    in_range = in_range && r[k] < a.in_dim[k];
-                }
-                if (!in_range) {
-                    if (lane == 0) atomicOr(a.err, 1u);
-                    continue;
-                }
-                orow[u] = o;
-                if (active) {
+                for (int k = 0; k < NIN; ++k) r[k] = __shfl_sync(0xffffffffu, my_r[q][k], src, G);
+                if (orow[u] != kNoRow && active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
                         f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)r[k] * a.stride, col);
@@ -331,28 +396,23 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (orow[u] == 0xFFFFFFFFu) continue;
-                if (orow[u] != cur) {
-                    if (cur != 0xFFFFFFFFu && active) flush(cur);
-#pragma unroll
-                    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
-                    cur = orow[u];
-                }
+                if (orow[u] == kNoRow) continue;
+                w.start(orow[u], a);
                 if (active) {
 #pragma unroll
                     for (int c = 0; c < CPL; ++c) {
                         float p = v[u] * f[u][0].at(c);
 #pragma unroll
                         for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
-                        acc[c] += p;
+                        w.acc[c] += p;
                     }
                 }
             }
         }
-        if (cur != 0xFFFFFFFFu && active) flush(cur);
-        __syncthreads();
-        zs = ze;
     }
+    const bool owner = w.finish(a);
+    __syncthreads();
+    if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
 }
 
 // COO schedule: packed records sorted by output index; no sorting in the kernel.
@@ -384,11 +444,15 @@ __global__ void __launch_bounds__(kSchedThreads, MINB) coo_sched_kernel(SchedArg
         }
         return;
     }
+    __shared__ uint32_t s_slot_row[kSchedThreads];
+    __shared__ uint8_t s_slot_whole[kSchedThreads];
+    float *s_slots = reinterpret_cast<float *>(sm + (size_t)kTile * RW * 4);  // [groups][G][CPL]
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
     const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;  // odd: groups start on different banks
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
-    process_records<G, CPL, U, NIN, FT>(s_rec, j0, j1, lane, a, a.vals ? a.vals + z0 : nullptr);
+    process_records<G, CPL, U, NIN, FT>(s_rec, n, j0, j1, g, lane, a, a.vals ? a.vals + z0 : nullptr, s_slots,
+                                        s_slot_row, s_slot_whole);
 }
 
 // ---------------------------------------------------------------------------
@@ -446,6 +510,25 @@ __global__ void nnz_keys_kernel(const uint32_t *blk, const uint32_t *inv, const 
         keys[z] = ((uint64_t)inv[blk[z]] << 8) | eout[z];
         vals[z] = (uint32_t)z;
     }
+}
+
+// Key of position j of the block order: (tile of j, output row of the nonzero).
+__global__ void tile_row_keys_kernel(const uint32_t *order, uint64_t n, const uint32_t *blk, const uint32_t *bout,
+                                     const uint8_t *eout, uint32_t sb, uint64_t *keys)
+{
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t z = order[j];
+        const uint32_t row = (bout[blk[z]] << sb) + eout[z];
+        keys[j] = ((j / (uint64_t)kHiTile) << 32) | row;
+    }
+}
+
+// Block of the nonzero at position j, counted from the first block of its tile.
+__global__ void local_block_kernel(const uint32_t *order, uint64_t n, const uint32_t *blk, const uint32_t *inv,
+                                   const uint32_t *tile_block, uint16_t *lblk)
+{
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+        lblk[j] = (uint16_t)(inv[blk[order[j]]] - tile_block[j / kHiTile]);
 }
 
 template <class T>
@@ -526,7 +609,7 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
     const uint64_t nb = t->nb;
     PTI_CHECK(t->sb <= 8, PTIERR_VALUE_ERROR, mod, "sb_bits must be <= 8");
     // 1. blocks by output-mode block coordinate (stable)
-    DevBuf bkeys, bperm, inv, bsize;
+    DevBuf bkeys, bperm, inv, bsize, nbptr;
     {
         RadixScratch rs;
         PTI_CUDA(bkeys.alloc(padded(nb * 8), s), mod);
@@ -542,13 +625,13 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
     PTI_CUDA(bsize.alloc(padded(nb * 4), s), mod);
     permuted_blocks_kernel<<<grid_n(nb), 256, 0, s>>>(bperm.as<uint32_t>(), nb, t->bptr.as<uint64_t>(),
                                                       bsize.as<uint32_t>(), inv.as<uint32_t>());
-    PTI_CUDA(P.bptr.alloc(padded((nb + 1) * 8), s), mod);
+    PTI_CUDA(nbptr.alloc(padded((nb + 1) * 8), s), mod);
     {
         DevBuf tmp;
         PTI_CUDA(tmp.alloc(padded(scan_tmp_elems<uint64_t>(nb) * 8), s), mod);
-        PTI_TRY((exclusive_scan<uint64_t>(SizeIn{bsize.as<uint32_t>()}, BptrOut{P.bptr.as<uint64_t>()}, nb,
+        PTI_TRY((exclusive_scan<uint64_t>(SizeIn{bsize.as<uint32_t>()}, BptrOut{nbptr.as<uint64_t>()}, nb,
                                           tmp.as<uint64_t>(), nullptr, s)));
-        PTI_CUDA(cudaMemcpyAsync(P.bptr.as<uint64_t>() + nb, tmp.as<uint64_t>() + (nb + kScanTile - 1) / kScanTile,
+        PTI_CUDA(cudaMemcpyAsync(nbptr.as<uint64_t>() + nb, tmp.as<uint64_t>() + (nb + kScanTile - 1) / kScanTile,
                                  8, cudaMemcpyDeviceToDevice, s), mod);
     }
     for (uint32_t k = 0; k < N; ++k) {
@@ -558,35 +641,44 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
     }
     bsize.reset();
     bperm.reset();
-    // 2. nonzeros: (new block, output offset), stable
-    {
-        DevBuf blk, zkeys, zperm;
-        RadixScratch rs;
-        PTI_CUDA(blk.alloc(padded(n * 4), s), mod);
-        block_of_nnz_kernel<<<grid_n(nb), 256, 0, s>>>(t->bptr.as<uint64_t>(), nb, blk.as<uint32_t>());
-        PTI_CUDA(zkeys.alloc(padded(n * 8), s), mod);
-        PTI_CUDA(zperm.alloc(padded(n * 4), s), mod);
-        nnz_keys_kernel<<<grid_n(n), 256, 0, s>>>(blk.as<uint32_t>(), inv.as<uint32_t>(),
-                                                  t->einds[mode].as<uint8_t>(), n, zkeys.as<uint64_t>(),
-                                                  zperm.as<uint32_t>());
-        blk.reset();
-        PTI_TRY(rs.alloc(n, s));
-        PTI_TRY(radix_sort_pairs(zkeys, zperm, n, (int)bits_for_count(nb) + 8, rs, s));
-        for (uint32_t k = 0; k < N; ++k) {
-            PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
-            gather_kernel<uint8_t><<<grid_n(n), 256, 0, s>>>(t->einds[k].as<uint8_t>(), zperm.as<uint32_t>(), n,
-                                                             P.einds[k].as<uint8_t>());
-        }
-        PTI_CUDA(P.vals.alloc(padded(n * 4), s), mod);
-        gather_kernel<float><<<grid_n(n), 256, 0, s>>>(t->vals.as<float>(), zperm.as<uint32_t>(), n,
-                                                       P.vals.as<float>());
-    }
-    inv.reset();
     P.nb = nb;
     P.ntiles = (uint32_t)((n + kHiTile - 1) / kHiTile);
     PTI_CUDA(P.tile_block.alloc(padded(((size_t)P.ntiles + 1) * 4), s), mod);
-    tile_block_kernel_t<<<grid_n(nb), 256, 0, s>>>(P.bptr.as<uint64_t>(), nb, P.ntiles, kHiTile,
+    tile_block_kernel_t<<<grid_n(nb), 256, 0, s>>>(nbptr.as<uint64_t>(), nb, P.ntiles, kHiTile,
                                                    P.tile_block.as<uint32_t>());
+    nbptr.reset();
+    {
+        // 2. nonzeros in block order: (new block, output offset), stable
+        DevBuf blk, keys, order;
+        RadixScratch rs;
+        PTI_CUDA(blk.alloc(padded(n * 4), s), mod);
+        block_of_nnz_kernel<<<grid_n(nb), 256, 0, s>>>(t->bptr.as<uint64_t>(), nb, blk.as<uint32_t>());
+        PTI_CUDA(keys.alloc(padded(n * 8), s), mod);
+        PTI_CUDA(order.alloc(padded(n * 4), s), mod);
+        nnz_keys_kernel<<<grid_n(n), 256, 0, s>>>(blk.as<uint32_t>(), inv.as<uint32_t>(),
+                                                  t->einds[mode].as<uint8_t>(), n, keys.as<uint64_t>(),
+                                                  order.as<uint32_t>());
+        PTI_TRY(rs.alloc(n, s));
+        PTI_TRY(radix_sort_pairs(keys, order, n, (int)bits_for_count(nb) + 8, rs, s));
+        // 3. inside each tile of that order: by output row, stable
+        tile_row_keys_kernel<<<grid_n(n), 256, 0, s>>>(order.as<uint32_t>(), n, blk.as<uint32_t>(),
+                                                       t->binds[mode].as<uint32_t>(), t->einds[mode].as<uint8_t>(),
+                                                       t->sb, keys.as<uint64_t>());
+        PTI_TRY(radix_sort_pairs(keys, order, n, 32 + (int)bits_for_count(P.ntiles), rs, s));
+        // 4. the nonzeros' encodings in that order
+        for (uint32_t k = 0; k < N; ++k) {
+            PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
+            gather_kernel<uint8_t><<<grid_n(n), 256, 0, s>>>(t->einds[k].as<uint8_t>(), order.as<uint32_t>(), n,
+                                                             P.einds[k].as<uint8_t>());
+        }
+        PTI_CUDA(P.vals.alloc(padded(n * 4), s), mod);
+        gather_kernel<float><<<grid_n(n), 256, 0, s>>>(t->vals.as<float>(), order.as<uint32_t>(), n,
+                                                       P.vals.as<float>());
+        PTI_CUDA(P.lblk.alloc(padded(n * 2), s), mod);
+        local_block_kernel<<<grid_n(n), 256, 0, s>>>(order.as<uint32_t>(), n, blk.as<uint32_t>(), inv.as<uint32_t>(),
+                                                     P.tile_block.as<uint32_t>(), P.lblk.as<uint16_t>());
+    }
+    inv.reset();
     PTI_CUDA(cudaGetLastError(), mod);
     P.ready = true;
     return 0;
@@ -598,7 +690,7 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
 template <int G, int CPL, int U, class FT, int NIN>
 static int launch_coo(const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
 {
-    const size_t smem = (size_t)kTile * Rec<NIN>::words * 4;
+    const size_t smem = (size_t)kTile * Rec<NIN>::words * 4 + (size_t)kSchedThreads * CPL * 4;
     auto k = coo_sched_kernel<G, CPL, U, 4, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
@@ -609,7 +701,7 @@ static int launch_coo(const SchedArgs &a, const uint32_t *recs, unsigned ntiles,
 template <int G, int CPL, class FT, int NIN>
 static int launch_hicoo(const SchedArgs &a, unsigned ntiles, cudaStream_t s)
 {
-    const size_t smem = HiSmem<NIN>::total;
+    const size_t smem = HiSmem<NIN, CPL>::total;
     auto k = hicoo_sched_kernel<G, CPL, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
@@ -695,7 +787,7 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
         ntiles = P.ntiles;
         a.nb = P.nb;
         a.sb = t->sb;
-        a.bptr = P.bptr.as<uint64_t>();
+        a.lblk = P.lblk.as<uint16_t>();
         a.tile_block = P.tile_block.as<uint32_t>();
         a.out_bind = P.binds[mode].as<uint32_t>();
         a.out_eind = P.einds[mode].as<uint8_t>();

@@ -12,20 +12,22 @@ constexpr int kMaxModes = 8;
 // Nonzeros per tile of a per-mode HiCOO schedule (HicooModePlan::tile_block).
 constexpr int kPlanTile = 2048;
 
-// Per-mode schedule of a HiCOO tensor: the blocks re-ordered by their block
-// coordinate in the output mode (a materialised form of the reference's
-// per-mode kernel scheduler kschr, src/sptensor/hicoo/convert.c:378-421), with
-// the nonzeros of each block re-ordered by their in-block output offset.  The
-// arrays use the HiCOO layout (bptr / binds / einds / values) so the same
-// kernels read them; `tiles` splits the nonzeros into nnz-balanced work items
-// that never split a block row's tile flush incorrectly (see mttkrp.cu).
+// Per-mode schedule of a HiCOO tensor.  The blocks are re-ordered by their
+// block coordinate in the output mode (a materialised form of the reference's
+// per-mode kernel scheduler kschr, src/sptensor/hicoo/convert.c:378-421) and
+// the nonzeros follow their blocks; the nonzeros are then cut into tiles of
+// kPlanTile, and inside each tile re-ordered by output row.  A nonzero keeps
+// its HiCOO encoding -- 8-bit element offsets per mode, plus the index of its
+// block among the tile's blocks (tile t covers blocks tile_block[t] ..
+// tile_block[t+1] of binds) -- so a tile is staged as it is and decoded
+// without sorting.
 struct HicooModePlan {
     bool ready = false;
     uint64_t nb = 0;
-    DevBuf bptr;                          // uint64 [nb+1]
-    std::array<DevBuf, kMaxModes> binds;  // uint32 [nb]
-    std::array<DevBuf, kMaxModes> einds;  // uint8  [nnz]
+    std::array<DevBuf, kMaxModes> binds;  // uint32 [nb]: block coordinates, blocks in output order
+    std::array<DevBuf, kMaxModes> einds;  // uint8  [nnz]: element offsets, tile-local row order
     DevBuf vals;                          // float  [nnz]
+    DevBuf lblk;                          // uint16 [nnz]: block of the nonzero - tile_block[tile]
     DevBuf tile_block;                    // uint32 [ntiles+1]: first block of each tile
     uint32_t ntiles = 0;
 };
