@@ -52,6 +52,7 @@ struct SchedArgs {
     uint32_t *err;
 };
 
+
 __device__ __forceinline__ uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
 
 // Words per packed nonzero record {output row, operand rows..., value},
@@ -228,12 +229,15 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
             if (orow[u] == kNoRow) continue;
             w.start(orow[u], a);
             if (active) {
+                const float2 vv = make_float2(val[u], val[u]);
 #pragma unroll
-                for (int c = 0; c < CPL; ++c) {
-                    float p = val[u] * f[u][0].at(c);
+                for (int c = 0; c < CPL; c += 2) {
+                    float2 p = make_float2(f[u][0].at(c), f[u][0].at(c + 1));
 #pragma unroll
-                    for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
-                    w.acc[c] += p;
+                    for (int k = 1; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[u][k].at(c), f[u][k].at(c + 1)));
+                    const float2 r = __ffma2_rn(p, vv, make_float2(w.acc[c], w.acc[c + 1]));
+                    w.acc[c] = r.x;
+                    w.acc[c + 1] = r.y;
                 }
             }
         }
@@ -254,6 +258,10 @@ struct HiSmem {
     static constexpr uint32_t bin = brow + 4 * (kHiTile + 4);           // u32[NIN][kHiTile + 4]
     static constexpr uint32_t slots = bin + 4 * NIN * (kHiTile + 4);    // float[kSchedThreads * CPL]
     static constexpr uint32_t total = slots + 4 * kSchedThreads * CPL;
+    // decoded records, written over the staged arrays once they are read
+    static constexpr uint32_t rec = 0;                                  // uint4[kHiTile]
+    static constexpr uint32_t rval = rec + 16 * kHiTile;                // float[kHiTile] (4-D only)
+    static_assert(rval + (NIN == 3 ? 4 * kHiTile : 0) <= slots, "records must fit over the staged tile");
 };
 
 // HiCOO schedule, one CTA per tile of kHiTile nonzeros.  The tile's nonzeros
@@ -267,7 +275,7 @@ template <int G, int CPL, class FT, int NIN>
 __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 {
     using L = HiSmem<NIN, CPL>;
-    constexpr int U = NIN <= 2 ? 4 : 2;  // nonzeros in flight per group
+    constexpr int U = NIN == 3 || CPL == 8 ? 2 : 3;  // nonzeros in flight per group
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t s_slot_row[kSchedThreads];
@@ -300,14 +308,14 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         const uint32_t be = round16(n), bv = round16(4 * n), bl = round16(2 * n);
         const uint32_t bb = 4 * ((nblk + bo4 + 3) & ~3u);
         mbar_arrive_expect_tx(&mbar, bv + (NIN + 1) * be + bl + (NIN + 1) * bb);
-        bulk_g2s(s_val, a.vals + z0, bv, &mbar);
-        bulk_g2s(s_eout, a.out_eind + z0, be, &mbar);
+        bulk_g2s_ef(s_val, a.vals + z0, bv, &mbar);
+        bulk_g2s_ef(s_eout, a.out_eind + z0, be, &mbar);
 #pragma unroll
-        for (int k = 0; k < NIN; ++k) bulk_g2s(s_ein + k * kHiTile, a.in_eind[k] + z0, be, &mbar);
-        bulk_g2s(s_blk, a.lblk + z0, bl, &mbar);
-        bulk_g2s(s_brow, a.out_bind + (b0 - bo4), bb, &mbar);
+        for (int k = 0; k < NIN; ++k) bulk_g2s_ef(s_ein + k * kHiTile, a.in_eind[k] + z0, be, &mbar);
+        bulk_g2s_ef(s_blk, a.lblk + z0, bl, &mbar);
+        bulk_g2s_ef(s_brow, a.out_bind + (b0 - bo4), bb, &mbar);
 #pragma unroll
-        for (int k = 0; k < NIN; ++k) bulk_g2s(s_bin + k * (kHiTile + 4), a.in_bind[k] + (b0 - bo4), bb, &mbar);
+        for (int k = 0; k < NIN; ++k) bulk_g2s_ef(s_bin + k * (kHiTile + 4), a.in_bind[k] + (b0 - bo4), bb, &mbar);
     }
     const bool ok = mbar_wait_bounded(&mbar, 0);
     if (!__syncthreads_and(ok)) {
@@ -320,26 +328,63 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
     s_brow += bo4;  // block i of the tile is entry i + bo4 of the staged coordinates
     s_bin += bo4;
 
+    // Decode every nonzero once into a 16-byte record {output row, operand
+    // rows} (the value in the last free word, or beside the records for
+    // 4-D), written over the staged arrays once they have all been read.
+    constexpr int PER = kHiTile / kSchedThreads;
+    {
+        uint4 rec[PER];
+        float vv[PER];
+#pragma unroll
+        for (int p = 0; p < PER; ++p) {
+            const uint32_t z = tid + p * kSchedThreads;
+            rec[p] = make_uint4(kNoRow, 0u, 0u, 0u);
+            vv[p] = 0.f;
+            if (z < n) {
+                const uint32_t i = s_blk[z];
+                const uint32_t o = (s_brow[i] << a.sb) + s_eout[z];
+                uint32_t r[3] = {0u, 0u, 0u};
+                bool ok_z = i < nblk && o < a.out_dim;
+#pragma unroll
+                for (int k = 0; k < NIN; ++k) {
+                    r[k] = (s_bin[k * (kHiTile + 4) + i] << a.sb) + s_ein[k * kHiTile + z];
+                    ok_z = ok_z && r[k] < a.in_dim[k];
+                }
+                vv[p] = s_val[z];
+                if (NIN == 1) r[1] = __float_as_uint(vv[p]);
+                if (NIN == 2) r[2] = __float_as_uint(vv[p]);
+                rec[p] = make_uint4(ok_z ? o : kNoRow, r[0], r[1], r[2]);
+                if (!ok_z) atomicOr(a.err, 1u);
+            }
+        }
+        __syncthreads();
+        uint4 *s_rec_w = reinterpret_cast<uint4 *>(sm + L::rec);
+        float *s_v3_w = reinterpret_cast<float *>(sm + L::rval);
+#pragma unroll
+        for (int p = 0; p < PER; ++p) {
+            const uint32_t z = tid + p * kSchedThreads;
+            if (z < n) {
+                s_rec_w[z] = rec[p];
+                if (NIN == 3) s_v3_w[z] = vv[p];
+            }
+        }
+    }
+    __syncthreads();
+    const uint4 *s_rec = reinterpret_cast<const uint4 *>(sm + L::rec);
+    const float *s_v3 = reinterpret_cast<const float *>(sm + L::rval);
+
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
-    // Each step a group decodes D nonzeros of its slice, Q per lane, and hands
-    // them to its lanes by shuffles.
-    constexpr int D = G >= U ? G : U;
-    constexpr int Q = D / G;
     const uint32_t col = lane * CPL;
     const bool active = col < a.R;
-    auto row_at = [&](uint32_t z) {
-        const uint32_t i = s_blk[z];
-        return i < nblk ? (s_brow[i] << a.sb) + s_eout[z] : kNoRow;
-    };
-    // an odd slice length puts the groups' first nonzeros on different shared-memory banks
+    // an odd slice length puts the groups' first records on different shared-memory banks
     const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
     bool first_shared = false, last_shared = false;
     if (j0 < j1) {
-        const uint32_t rf = row_at(j0), rl = row_at(j1 - 1);
-        first_shared = j0 > 0 && row_at(j0 - 1) == rf;
-        last_shared = j1 < n && row_at(j1) == rl;
+        const uint32_t rf = s_rec[j0].x, rl = s_rec[j1 - 1].x;
+        first_shared = j0 > 0 && s_rec[j0 - 1].x == rf;
+        last_shared = j1 < n && s_rec[j1].x == rl;
         if (lane == 0) {
             s_slot_row[g] = first_shared ? rf : kNoRow;
             s_slot_whole[g] = rf == rl;
@@ -349,63 +394,39 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         s_slot_whole[g] = 0;
     }
     RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
-    const uint32_t nsteps = (per + D - 1) / D;  // the same for every group: shuffles stay warp-uniform
-    for (uint32_t step = 0; step < nsteps; ++step) {
-        const uint32_t jb = j0 + step * D;
-        uint32_t my_o[Q], my_r[Q][NIN];
-        float my_v[Q];
+    for (uint32_t j = j0; j < j1; j += U) {
+        uint32_t orow[U];
+        float v[U];
+        RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const uint32_t z = jb + q * G + lane;
-            my_o[q] = kNoRow;
-            my_v[q] = 0.f;
-#pragma unroll
-            for (int k = 0; k < NIN; ++k) my_r[q][k] = 0;
-            if (z < j1) {
-                const uint32_t i = s_blk[z];
-                const uint32_t o = (s_brow[i] << a.sb) + s_eout[z];
-                bool ok_z = i < nblk && o < a.out_dim;
-#pragma unroll
-                for (int k = 0; k < NIN; ++k) {
-                    my_r[q][k] = (s_bin[k * (kHiTile + 4) + i] << a.sb) + s_ein[k * kHiTile + z];
-                    ok_z = ok_z && my_r[q][k] < a.in_dim[k];
-                }
-                my_v[q] = s_val[z];
-                if (ok_z) my_o[q] = o;
-                else atomicOr(a.err, 1u);
-            }
-        }
-#pragma unroll
-        for (int t0 = 0; t0 < D; t0 += U) {
-            uint32_t orow[U];
-            float v[U];
-            RowPart<CPL, FT> f[U][NIN];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int t = t0 + u, src = t % G, q = t / G;
-                orow[u] = __shfl_sync(0xffffffffu, my_o[q], src, G);
-                v[u] = __shfl_sync(0xffffffffu, my_v[q], src, G);
-                uint32_t r[NIN];
-#pragma unroll
-                for (int k = 0; k < NIN; ++k) r[k] = __shfl_sync(0xffffffffu, my_r[q][k], src, G);
+        for (int u = 0; u < U; ++u) {
+            orow[u] = kNoRow;
+            if (j + u < j1) {
+                const uint4 r = s_rec[j + u];
+                const uint32_t rr[3] = {r.y, r.z, r.w};
+                orow[u] = r.x;
+                v[u] = NIN == 3 ? s_v3[j + u] : __uint_as_float(NIN == 2 ? r.w : r.z);
                 if (orow[u] != kNoRow && active) {
 #pragma unroll
                     for (int k = 0; k < NIN; ++k)
-                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)r[k] * a.stride, col);
+                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)rr[k] * a.stride, col);
                 }
             }
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (orow[u] == kNoRow) continue;
-                w.start(orow[u], a);
-                if (active) {
+        for (int u = 0; u < U; ++u) {
+            if (orow[u] == kNoRow) continue;
+            w.start(orow[u], a);
+            if (active) {
+                const float2 vv = make_float2(v[u], v[u]);
 #pragma unroll
-                    for (int c = 0; c < CPL; ++c) {
-                        float p = v[u] * f[u][0].at(c);
+                for (int c = 0; c < CPL; c += 2) {
+                    float2 p = make_float2(f[u][0].at(c), f[u][0].at(c + 1));
 #pragma unroll
-                        for (int k = 1; k < NIN; ++k) p *= f[u][k].at(c);
-                        w.acc[c] += p;
-                    }
+                    for (int k = 1; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[u][k].at(c), f[u][k].at(c + 1)));
+                    const float2 q = __ffma2_rn(p, vv, make_float2(w.acc[c], w.acc[c + 1]));
+                    w.acc[c] = q.x;
+                    w.acc[c + 1] = q.y;
                 }
             }
         }
@@ -434,7 +455,7 @@ __global__ void __launch_bounds__(kSchedThreads, MINB) coo_sched_kernel(SchedArg
     if (tid == 0) {
         const uint32_t bytes = n * RW * 4;
         mbar_arrive_expect_tx(&mbar, bytes);
-        bulk_g2s(s_rec, recs + z0 * RW, bytes, &mbar);
+        bulk_g2s_ef(s_rec, recs + z0 * RW, bytes, &mbar);
     }
     const bool ok = mbar_wait_bounded(&mbar, 0);
     if (!__syncthreads_and(ok)) {
