@@ -54,6 +54,7 @@ namespace pti {
 
 constexpr int kBThreads = 256;
 constexpr int kBMaxRank = 32;
+constexpr int kRowPad = 40;                     // row stride (doubles) of the dense passes' row tiles
 constexpr int kBTile = kPlanTile;
 constexpr uint64_t kWaitNs = 2000000000ull;     // bound of every dependency wait: 2 s
 
@@ -177,7 +178,9 @@ struct TileSmem {
 struct DenseSmem {
     static constexpr uint32_t RR = kBMaxRank * kBMaxRank;
     static constexpr uint32_t V = 0, L = V + 8 * RR, Li = L + 8 * RR, W = Li + 8 * RR, Gs = W + 8 * RR;
-    static constexpr uint32_t colsq = Gs + 8 * RR;              // double[32]
+    static constexpr uint32_t Wf = Gs + 8 * RR;                 // double[8 k-steps][4 n-tiles][32 lanes]
+    static constexpr uint32_t rows = Wf + 8 * RR;               // double[warps][8][kRowPad]
+    static constexpr uint32_t colsq = rows + 8 * (kBThreads / 32) * 8 * kRowPad;  // double[32]
     static constexpr uint32_t red = colsq + 8 * kBMaxRank;      // double[kBThreads/32 + 1]
     static constexpr uint32_t lam = red + 8 * (kBThreads / 32 + 1);  // float[32]
     static constexpr uint32_t colmax = lam + 4 * kBMaxRank;     // int[32]
@@ -185,6 +188,15 @@ struct DenseSmem {
 };
 
 constexpr uint32_t kBatchSmem = TileSmem::total > DenseSmem::total ? TileSmem::total : DenseSmem::total;
+
+// D += A B for one 8x8x4 FP64 tensor-core tile (mma.sync m8n8k4): lane l holds
+// A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
 
 __device__ __forceinline__ uint32_t round16u(uint32_t x) { return (x + 15u) & ~15u; }
 
@@ -478,34 +490,86 @@ __device__ void dense_task(const BatchTensor *__restrict__ gt, uint32_t b, uint3
     __syncthreads();
     spd_inverse(V, Lm, Li, W, R);
 
-    // pass 1: A = M W (FP64), column sums of squares and maxima
+    // B operands of pass 1 in fragment order: Wf[kt][nt][lane] = W[4kt + lane%4][8nt + lane/4]
+    double *Wf = reinterpret_cast<double *>(sm + DenseSmem::Wf);
+    for (uint32_t e = tid; e < 8 * 4 * 32; e += kBThreads) {
+        const uint32_t l = e & 31, nt = (e >> 5) & 3, kt = e >> 7;
+        const uint32_t k = 4 * kt + (l & 3), c = 8 * nt + (l >> 2);
+        Wf[e] = (k < R && c < R) ? W[k * R + c] : 0.0;
+    }
+    __syncthreads();
+
+    // The passes run on the FP64 tensor cores (mma.sync m8n8k4), one warp per
+    // block of 8 rows; lane l is (g, t) = (l/4, l%4).
+    const uint32_t g8 = lane >> 2, t4 = lane & 3;
+    const uint32_t KT = (R + 3) / 4, NT = (R + 7) / 8;  // k-steps and 8-column tiles (NT * 8 == stride)
+    const uint32_t nblk8 = (I + 7) / 8;
     const bool colok = lane < R;
+
+    // pass 1: A = M W, with column sums of squares and maxima
     {
-        double wc[kBMaxRank];
+        double csq[8];
+        float cmx[8];
 #pragma unroll
-        for (int k = 0; k < kBMaxRank; ++k) wc[k] = (colok && k < (int)R) ? W[k * R + lane] : 0.0;
-        double csq = 0.0;
-        float cmx = 0.f;
-        for (uint32_t i = warp; i < I; i += kWarps) {
-            const float mv = colok ? __ldcg(M + (size_t)i * stride + lane) : 0.f;
-            double s = 0.0;
+        for (int j = 0; j < 8; ++j) {
+            csq[j] = 0.0;
+            cmx[j] = 0.f;
+        }
+        float anext[8];
+        auto load_a = [&](uint32_t blk, float (&av)[8]) {
+            const uint32_t row = blk * 8 + g8;
 #pragma unroll
-            for (int k = 0; k < kBMaxRank; ++k) {
-                if (k < (int)R) {
-                    const float mk = __shfl_sync(0xffffffffu, mv, k);
-                    s = fma((double)mk, wc[k], s);
+            for (int kt = 0; kt < 8; ++kt) {
+                const uint32_t k = 4 * kt + t4;
+                av[kt] = (blk < nblk8 && row < I && k < R) ? __ldcg(M + (size_t)row * stride + k) : 0.f;
+            }
+        };
+        uint32_t blk = warp;
+        load_a(blk, anext);
+        for (; blk < nblk8; blk += kWarps) {
+            float av[8];
+#pragma unroll
+            for (int kt = 0; kt < 8; ++kt) av[kt] = anext[kt];
+            load_a(blk + kWarps, anext);
+            double c[4][2];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) c[nt][0] = c[nt][1] = 0.0;
+#pragma unroll
+            for (int kt = 0; kt < 8; ++kt) {
+                if (kt < (int)KT) {
+                    const double a = (double)av[kt];
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt)
+                        if (nt < (int)NT) dmma(c[nt][0], c[nt][1], a, Wf[(kt * 4 + nt) * 32 + lane]);
                 }
             }
-            const float v = (float)s;
-            if (lane < stride) A[(size_t)i * stride + lane] = colok ? v : 0.f;
-            if (colok) {
-                csq += (double)v * (double)v;
-                cmx = fmaxf(cmx, v);
+            const uint32_t row = blk * 8 + g8;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                if (nt >= (int)NT) break;
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const uint32_t col = 8 * nt + 2 * t4 + i;
+                    const float v = col < R ? (float)c[nt][i] : 0.f;
+                    if (row < I) {
+                        A[(size_t)row * stride + col] = v;
+                        csq[2 * nt + i] += (double)v * (double)v;
+                        cmx[2 * nt + i] = fmaxf(cmx[2 * nt + i], v);
+                    }
+                }
             }
         }
-        if (colok) {
-            atomicAdd(&s_colsq[lane], csq);
-            atomicMax(&s_colmax[lane], __float_as_int(cmx));
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            if (nt >= (int)NT) break;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t col = 8 * nt + 2 * t4 + i;
+                if (col < R) {
+                    atomicAdd(&s_colsq[col], csq[2 * nt + i]);
+                    atomicMax(&s_colmax[col], __float_as_int(cmx[2 * nt + i]));
+                }
+            }
         }
     }
     __syncthreads();
@@ -516,29 +580,72 @@ __device__ void dense_task(const BatchTensor *__restrict__ gt, uint32_t b, uint3
                             : 1.f;
     if (warp == 0 && colok) s_lam[lane] = lam;
 
-    // pass 2: A /= lambda, BF16 copy, Gram, and <X, model> for the fit
+    // pass 2: A /= lambda, BF16 copy, <X, model> for the fit, and the Gram
+    // A^T A on the tensor cores: the warp's 8 scaled rows go through a
+    // shared-memory tile, each half (4 rows) is one k-step for the tiles
+    // (p, q), p <= q, of the symmetric Gram.
     const bool last = m == 2;
     double inner = 0.0;
     {
-        double g[kBMaxRank];
+        double *tile = reinterpret_cast<double *>(sm + DenseSmem::rows) + warp * (8 * kRowPad);
+        double gacc[10][2];
 #pragma unroll
-        for (int k = 0; k < kBMaxRank; ++k) g[k] = 0.0;
-        for (uint32_t i = warp; i < I; i += kWarps) {
-            const size_t e = (size_t)i * stride + lane;
-            float v = 0.f;
-            if (colok) {
-                v = A[e] / lam;
-                A[e] = v;
-                if (last) inner += (double)lam * (double)v * (double)__ldcg(M + e);
+        for (int j = 0; j < 10; ++j) gacc[j][0] = gacc[j][1] = 0.0;
+        for (uint32_t blk = warp; blk < nblk8; blk += kWarps) {
+            float v[8], mm[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t row = blk * 8 + q;
+                const bool here = colok && row < I;
+                v[q] = here ? A[(size_t)row * stride + lane] : 0.f;
+                mm[q] = here && last ? __ldcg(M + (size_t)row * stride + lane) : 0.f;
             }
-            if (a.mixed && lane < stride) Ab[e] = __float2bfloat16_rn(v);
-            gram_row(g, v, R);
-        }
-        if (colok) {
+            __syncwarp();
 #pragma unroll
-            for (int k = 0; k < kBMaxRank; ++k)
-                if (k < (int)R) atomicAdd(&Gs[lane * R + k], g[k]);
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t row = blk * 8 + q;
+                if (colok) {
+                    v[q] = v[q] / lam;
+                    if (row < I) {
+                        A[(size_t)row * stride + lane] = v[q];
+                        if (last) inner += (double)lam * (double)v[q] * (double)mm[q];
+                    }
+                }
+                if (a.mixed && lane < stride && row < I)
+                    Ab[(size_t)row * stride + lane] = __float2bfloat16_rn(colok ? v[q] : 0.f);
+                tile[q * kRowPad + lane] = (double)v[q];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                double fr[4];
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) fr[nt] = tile[(4 * ks + t4) * kRowPad + 8 * nt + g8];
+                int j = 0;
+#pragma unroll
+                for (int pt = 0; pt < 4; ++pt)
+#pragma unroll
+                    for (int qt = pt; qt < 4; ++qt, ++j)
+                        if (qt < (int)NT) dmma(gacc[j][0], gacc[j][1], fr[pt], fr[qt]);
+            }
+            __syncwarp();
         }
+        // add the warp's tiles into the Gram: tile (p, q) holds G[8p + g][8q + 2t + i]
+        int j = 0;
+#pragma unroll
+        for (int pt = 0; pt < 4; ++pt)
+#pragma unroll
+            for (int qt = pt; qt < 4; ++qt, ++j) {
+                if (qt >= (int)NT) continue;
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const uint32_t r = 8 * pt + g8, c = 8 * qt + 2 * t4 + i;
+                    if (r < R && c < R) {
+                        atomicAdd(&Gs[r * R + c], gacc[j][i]);
+                        if (pt != qt) atomicAdd(&Gs[c * R + r], gacc[j][i]);
+                    }
+                }
+            }
     }
     // zero the next mode's MTTKRP output (its tiles wait for this step)
     {
