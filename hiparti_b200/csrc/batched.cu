@@ -171,7 +171,8 @@ struct TileSmem {
     static constexpr uint32_t blk = ein + 2 * kBTile;           // u16[kBTile]
     static constexpr uint32_t brow = blk + 2 * kBTile;          // u32[kBTile + 4]
     static constexpr uint32_t bin = brow + 4 * (kBTile + 4);    // u32[2][kBTile + 4]
-    static constexpr uint32_t total = bin + 8 * (kBTile + 4);
+    static constexpr uint32_t rec = bin + 8 * (kBTile + 4);     // u32[3][kBTile]: decoded output and operand rows
+    static constexpr uint32_t total = rec + 12 * kBTile;
 };
 
 // Shared-memory layout of a dense task (doubles unless noted).
@@ -188,6 +189,7 @@ struct DenseSmem {
 };
 
 constexpr uint32_t kBatchSmem = TileSmem::total > DenseSmem::total ? TileSmem::total : DenseSmem::total;
+static_assert(TileSmem::rec % 16 == 0 && kBatchSmem <= 76 * 1024, "three CTAs per SM must fit");
 
 // D += A B for one 8x8x4 FP64 tensor-core tile (mma.sync m8n8k4): lane l holds
 // A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1].
@@ -233,14 +235,14 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
         const uint32_t be = round16u(n), bv = round16u(4 * n), bl = round16u(2 * n);
         const uint32_t bb = 4 * ((nblk + bo4 + 3) & ~3u);
         mbar_arrive_expect_tx(mbar, bv + 3 * be + bl + 3 * bb);
-        bulk_g2s(s_val, gp->vals + z0, bv, mbar);
-        bulk_g2s(s_eout, gp->out_eind + z0, be, mbar);
-        bulk_g2s(s_ein, gp->in_eind[0] + z0, be, mbar);
-        bulk_g2s(s_ein + kBTile, gp->in_eind[1] + z0, be, mbar);
-        bulk_g2s(s_blk, gp->lblk + z0, bl, mbar);
-        bulk_g2s(s_brow, gp->out_bind + (b0 - bo4), bb, mbar);
-        bulk_g2s(s_bin, gp->in_bind[0] + (b0 - bo4), bb, mbar);
-        bulk_g2s(s_bin + (kBTile + 4), gp->in_bind[1] + (b0 - bo4), bb, mbar);
+        bulk_g2s_ef(s_val, gp->vals + z0, bv, mbar);
+        bulk_g2s_ef(s_eout, gp->out_eind + z0, be, mbar);
+        bulk_g2s_ef(s_ein, gp->in_eind[0] + z0, be, mbar);
+        bulk_g2s_ef(s_ein + kBTile, gp->in_eind[1] + z0, be, mbar);
+        bulk_g2s_ef(s_blk, gp->lblk + z0, bl, mbar);
+        bulk_g2s_ef(s_brow, gp->out_bind + (b0 - bo4), bb, mbar);
+        bulk_g2s_ef(s_bin, gp->in_bind[0] + (b0 - bo4), bb, mbar);
+        bulk_g2s_ef(s_bin + (kBTile + 4), gp->in_bind[1] + (b0 - bo4), bb, mbar);
     }
     const bool ok = mbar_wait_bounded(mbar, phase);
     phase ^= 1u;
@@ -250,6 +252,22 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
     }
     s_brow += bo4;
     s_bin += bo4;
+    // decode every nonzero once: output row (or a marker for a bad
+    // coordinate) and operand rows, into shared memory beside the tile
+    uint32_t *s_ro = reinterpret_cast<uint32_t *>(sm + TileSmem::rec);
+    uint32_t *s_r0 = s_ro + kBTile, *s_r1 = s_r0 + kBTile;
+    for (uint32_t z = tid; z < n; z += kBThreads) {
+        const uint32_t i = s_blk[z];
+        const uint32_t o = (s_brow[i] << sb) + s_eout[z];
+        const uint32_t r0 = (s_bin[i] << sb) + s_ein[z];
+        const uint32_t r1 = (s_bin[(kBTile + 4) + i] << sb) + s_ein[kBTile + z];
+        const bool ok_z = i < nblk && o < out_dim && r0 < in_dim0 && r1 < in_dim1;
+        if (!ok_z) atomicOr(err, kErrRange);
+        s_ro[z] = ok_z ? o : 0xFFFFFFFFu;
+        s_r0[z] = r0;
+        s_r1[z] = r1;
+    }
+    __syncthreads();
 
     const FT *mat0, *mat1;
     if constexpr (sizeof(FT) == 4) {
@@ -289,19 +307,12 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
         for (int u = 0; u < U; ++u) {
             orow[u] = 0xFFFFFFFFu;
             if (j + u >= j1) continue;
-            const uint32_t z = j + u, i = s_blk[z];
-            const uint32_t o = (s_brow[i] << sb) + s_eout[z];
-            const uint32_t r0 = (s_bin[i] << sb) + s_ein[z];
-            const uint32_t r1 = (s_bin[(kBTile + 4) + i] << sb) + s_ein[kBTile + z];
+            const uint32_t z = j + u;
+            orow[u] = s_ro[z];
             v[u] = s_val[z];
-            if (!(i < nblk && o < out_dim && r0 < in_dim0 && r1 < in_dim1)) {
-                if (lane == 0) atomicOr(err, kErrRange);
-                continue;
-            }
-            orow[u] = o;
-            if (active) {
-                f0[u].load(mat0 + (size_t)r0 * stride, col);
-                f1[u].load(mat1 + (size_t)r1 * stride, col);
+            if (orow[u] != 0xFFFFFFFFu && active) {
+                f0[u].load(mat0 + (size_t)s_r0[z] * stride, col);
+                f1[u].load(mat1 + (size_t)s_r1[z] * stride, col);
             }
         }
 #pragma unroll
