@@ -20,6 +20,7 @@
 // ssyrk_ call does not write, so its printed fit is not the model's fit.)
 #include <cuda_bf16.h>
 
+#include "spd.cuh"
 #include "tensor.cuh"
 
 namespace pti {
@@ -68,9 +69,27 @@ __global__ void gram_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, c
     for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) atomicAdd(G + e, acc[e]);
 }
 
-// One CTA: W = (Hadamard_{k != mode} G_k)^{-1}.  work holds 3*R*R doubles.
-// flag[0] = 1 if the Cholesky factorisation failed (fallback used), 2 if the
-// matrix was singular (W = identity: rows left unsolved).
+// One CTA: W = (Hadamard_{k != mode} G_k)^{-1}.  flag[0] = 1 if the Cholesky
+// factorisation failed (fallback used), 2 if the matrix was singular
+// (W = identity: rows left unsolved).  Ranks up to 32: the matrices sit in
+// shared memory and one warp factors them (spd_inverse).
+__global__ void gram_inverse_small_kernel(const double *G, uint32_t N, uint32_t R, uint32_t mode, double *W,
+                                          int *flag)
+{
+    __shared__ double sV[32 * 32], sL[32 * 32], sLi[32 * 32], sW[32 * 32];
+    const uint32_t RR = R * R;
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
+        double v = 1.0;
+        for (uint32_t k = 1; k < N; ++k) v *= G[(size_t)((mode + k) % N) * RR + e];
+        sV[e] = v;
+    }
+    __syncthreads();
+    const int f = spd_inverse(sV, sL, sLi, sW, R);
+    for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) W[e] = sW[e];
+    if (threadIdx.x == 0) flag[0] = f;
+}
+
+// The same for ranks above 32; work holds 3*R*R doubles in global memory.
 __global__ void gram_inverse_kernel(const double *G, uint32_t N, uint32_t R, uint32_t mode, double *W,
                                     double *work, int *flag)
 {
@@ -383,7 +402,11 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
             for (uint32_t i = 0; i < N; ++i) order[i] = (m + i) % N;
             PTI_TRY(mttkrp_device(t, fptr.data(), use_bf16 ? PTI_B200_BF16 : PTI_B200_F32, R, stride, order.data(), m,
                                   M.as<float>(), s));
-            gram_inverse_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), work.as<double>(), flag);
+            if (R <= 32)
+                gram_inverse_small_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), flag);
+            else
+                gram_inverse_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), work.as<double>(),
+                                                      flag);
             PTI_CUDA(cudaMemsetAsync(stats.ptr, 0, (size_t)R * 12, s), mod);
             solve_rows_kernel<<<rows_grid((uint64_t)t->ndims[m] * stride, 256), 256, solve_smem, s>>>(
                 M.as<float>(), W.as<double>(), t->ndims[m], R, stride, A[m], colsq, colmax);

@@ -79,6 +79,12 @@ struct RowPart {
             raw = make_uint4(r.x, r.y, 0u, 0u);
         }
     }
+    // 32-bit word i of the loaded columns
+    __device__ __forceinline__ uint32_t word(int i) const
+    {
+        const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
+        return w[i];
+    }
     // column c (0 <= c < CPL) as FP32
     __device__ __forceinline__ float at(int c) const
     {
@@ -91,6 +97,46 @@ struct RowPart {
         }
     }
 };
+
+// Exact FP32 products of the two BF16 halves of a and b (a mixed-precision
+// FMA with a zero addend; a product of two BF16 values is exact in FP32).
+__device__ __forceinline__ float2 bf16x2_mul(uint32_t a, uint32_t b)
+{
+    float lo, hi;
+    asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t"
+        "mov.b32 {al, ah}, %2;\n\t"
+        "mov.b32 {bl, bh}, %3;\n\t"
+        "fma.rn.f32.bf16 %0, al, bl, 0f00000000;\n\t"
+        "fma.rn.f32.bf16 %1, ah, bh, 0f00000000;\n\t}"
+        : "=f"(lo), "=f"(hi)
+        : "r"(a), "r"(b));
+    return make_float2(lo, hi);
+}
+
+// acc[c] += v * prod_k f[k][c] for the CPL columns of a lane, with packed
+// FP32x2 arithmetic; BF16 rows multiply their first two factors exactly in
+// FP32 without unpacking them.
+template <int CPL, class FT, int NIN>
+__device__ __forceinline__ void accumulate(float *acc, const RowPart<CPL, FT> (&f)[NIN], float v)
+{
+    const float2 vv = make_float2(v, v);
+#pragma unroll
+    for (int c = 0; c < CPL; c += 2) {
+        float2 p;
+        if constexpr (sizeof(FT) == 2 && NIN >= 2) {
+            p = bf16x2_mul(f[0].word(c >> 1), f[1].word(c >> 1));
+#pragma unroll
+            for (int k = 2; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[k].at(c), f[k].at(c + 1)));
+        } else {
+            p = make_float2(f[0].at(c), f[0].at(c + 1));
+#pragma unroll
+            for (int k = 1; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[k].at(c), f[k].at(c + 1)));
+        }
+        const float2 r = __ffma2_rn(p, vv, make_float2(acc[c], acc[c + 1]));
+        acc[c] = r.x;
+        acc[c + 1] = r.y;
+    }
+}
 
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 
@@ -228,18 +274,7 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
         for (int u = 0; u < U; ++u) {
             if (orow[u] == kNoRow) continue;
             w.start(orow[u], a);
-            if (active) {
-                const float2 vv = make_float2(val[u], val[u]);
-#pragma unroll
-                for (int c = 0; c < CPL; c += 2) {
-                    float2 p = make_float2(f[u][0].at(c), f[u][0].at(c + 1));
-#pragma unroll
-                    for (int k = 1; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[u][k].at(c), f[u][k].at(c + 1)));
-                    const float2 r = __ffma2_rn(p, vv, make_float2(w.acc[c], w.acc[c + 1]));
-                    w.acc[c] = r.x;
-                    w.acc[c + 1] = r.y;
-                }
-            }
+            if (active) accumulate<CPL, FT, NIN>(w.acc, f[u], val[u]);
         }
     }
     const bool owner = w.finish(a);
@@ -417,18 +452,7 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         for (int u = 0; u < U; ++u) {
             if (orow[u] == kNoRow) continue;
             w.start(orow[u], a);
-            if (active) {
-                const float2 vv = make_float2(v[u], v[u]);
-#pragma unroll
-                for (int c = 0; c < CPL; c += 2) {
-                    float2 p = make_float2(f[u][0].at(c), f[u][0].at(c + 1));
-#pragma unroll
-                    for (int k = 1; k < NIN; ++k) p = __fmul2_rn(p, make_float2(f[u][k].at(c), f[u][k].at(c + 1)));
-                    const float2 q = __ffma2_rn(p, vv, make_float2(w.acc[c], w.acc[c + 1]));
-                    w.acc[c] = q.x;
-                    w.acc[c + 1] = q.y;
-                }
-            }
+            if (active) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
         }
     }
     const bool owner = w.finish(a);
