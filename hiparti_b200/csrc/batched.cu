@@ -326,8 +326,16 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
                 cur = orow[u];
             }
             if (active) {
+                const float2 vv = make_float2(v[u], v[u]);
 #pragma unroll
-                for (int c = 0; c < CPL; ++c) acc[c] += v[u] * f0[u].at(c) * f1[u].at(c);
+                for (int c = 0; c < CPL; c += 2) {
+                    float2 p;
+                    if constexpr (sizeof(FT) == 2) p = bf16x2_mul(f0[u].w[c >> 1], f1[u].w[c >> 1]);
+                    else p = __fmul2_rn(make_float2(f0[u].at(c), f0[u].at(c + 1)), make_float2(f1[u].at(c), f1[u].at(c + 1)));
+                    const float2 r = __ffma2_rn(p, vv, make_float2(acc[c], acc[c + 1]));
+                    acc[c] = r.x;
+                    acc[c + 1] = r.y;
+                }
             }
         }
     }

@@ -50,4 +50,19 @@ __device__ __forceinline__ float4 mask4(float4 v, uint32_t col, uint32_t R)
                        col + 3 < R ? v.w : 0.f);
 }
 
+// Exact FP32 products of the two BF16 halves of a and b (a mixed-precision
+// FMA with a zero addend; a product of two BF16 values is exact in FP32).
+__device__ __forceinline__ float2 bf16x2_mul(uint32_t a, uint32_t b)
+{
+    float lo, hi;
+    asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t"
+        "mov.b32 {al, ah}, %2;\n\t"
+        "mov.b32 {bl, bh}, %3;\n\t"
+        "fma.rn.f32.bf16 %0, al, bl, 0f00000000;\n\t"
+        "fma.rn.f32.bf16 %1, ah, bh, 0f00000000;\n\t}"
+        : "=f"(lo), "=f"(hi)
+        : "r"(a), "r"(b));
+    return make_float2(lo, hi);
+}
+
 }  // namespace pti

@@ -98,21 +98,6 @@ struct RowPart {
     }
 };
 
-// Exact FP32 products of the two BF16 halves of a and b (a mixed-precision
-// FMA with a zero addend; a product of two BF16 values is exact in FP32).
-__device__ __forceinline__ float2 bf16x2_mul(uint32_t a, uint32_t b)
-{
-    float lo, hi;
-    asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t"
-        "mov.b32 {al, ah}, %2;\n\t"
-        "mov.b32 {bl, bh}, %3;\n\t"
-        "fma.rn.f32.bf16 %0, al, bl, 0f00000000;\n\t"
-        "fma.rn.f32.bf16 %1, ah, bh, 0f00000000;\n\t}"
-        : "=f"(lo), "=f"(hi)
-        : "r"(a), "r"(b));
-    return make_float2(lo, hi);
-}
-
 // acc[c] += v * prod_k f[k][c] for the CPL columns of a lane, with packed
 // FP32x2 arithmetic; BF16 rows multiply their first two factors exactly in
 // FP32 without unpacking them.
@@ -548,24 +533,53 @@ __global__ void permuted_blocks_kernel(const uint32_t *perm, uint64_t nb, const 
     }
 }
 
-__global__ void nnz_keys_kernel(const uint32_t *blk, const uint32_t *inv, const uint8_t *eout, uint64_t n,
-                                uint64_t *keys, uint32_t *vals)
+// Position of every nonzero in block order (blocks in their new order, the
+// nonzeros of a block in their stored order): order[pos] = z.
+__global__ void block_order_kernel(const uint32_t *blk, const uint32_t *inv, const uint64_t *bptr,
+                                   const uint64_t *nbptr, uint64_t n, uint32_t *order)
 {
     for (uint64_t z = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (uint64_t)gridDim.x * blockDim.x) {
-        keys[z] = ((uint64_t)inv[blk[z]] << 8) | eout[z];
-        vals[z] = (uint32_t)z;
+        const uint32_t b = blk[z];
+        order[nbptr[inv[b]] + (z - bptr[b])] = (uint32_t)z;
     }
 }
 
-// Key of position j of the block order: (tile of j, output row of the nonzero).
-__global__ void tile_row_keys_kernel(const uint32_t *order, uint64_t n, const uint32_t *blk, const uint32_t *bout,
-                                     const uint8_t *eout, uint32_t sb, uint64_t *keys)
+// One CTA per tile of the block order: stable sort of the tile's nonzeros by
+// output row (a bitonic sort of (row, position) pairs in shared memory).
+__global__ void __launch_bounds__(256) tile_sort_kernel(const uint32_t *order, uint64_t n, const uint32_t *blk,
+                                                        const uint32_t *bout, const uint8_t *eout, uint32_t sb,
+                                                        uint32_t *sorted)
 {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t z = order[j];
-        const uint32_t row = (bout[blk[z]] << sb) + eout[z];
-        keys[j] = ((j / (uint64_t)kHiTile) << 32) | row;
+    constexpr uint32_t T = kHiTile;
+    static_assert((T & (T - 1)) == 0 && T <= 4096, "tile must be a power of two of at most 4096");
+    __shared__ uint64_t key[T];
+    const uint64_t z0 = (uint64_t)blockIdx.x * T;
+    const uint32_t cnt = (uint32_t)((n - z0) < T ? (n - z0) : T);
+    for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) {
+        if (i < cnt) {
+            const uint32_t z = order[z0 + i];
+            const uint64_t row = ((uint64_t)bout[blk[z]] << sb) + eout[z];
+            key[i] = (row << 12) | i;
+        } else {
+            key[i] = ~0ull;  // padding sorts last
+        }
     }
+    __syncthreads();
+    for (uint32_t k = 2; k <= T; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const uint64_t x = key[i], y = key[ixj];
+                    if ((x > y) == ((i & k) == 0)) {
+                        key[i] = y;
+                        key[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) sorted[z0 + i] = order[z0 + (uint32_t)(key[i] & 4095u)];
 }
 
 // Block of the nonzero at position j, counted from the first block of its tile.
@@ -691,25 +705,20 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
     PTI_CUDA(P.tile_block.alloc(padded(((size_t)P.ntiles + 1) * 4), s), mod);
     tile_block_kernel_t<<<grid_n(nb), 256, 0, s>>>(nbptr.as<uint64_t>(), nb, P.ntiles, kHiTile,
                                                    P.tile_block.as<uint32_t>());
-    nbptr.reset();
     {
-        // 2. nonzeros in block order: (new block, output offset), stable
-        DevBuf blk, keys, order;
-        RadixScratch rs;
+        // 2. nonzeros in block order (blocks in their new order), then 3. inside
+        // each tile of that order by output row
+        DevBuf blk, border, order;
         PTI_CUDA(blk.alloc(padded(n * 4), s), mod);
         block_of_nnz_kernel<<<grid_n(nb), 256, 0, s>>>(t->bptr.as<uint64_t>(), nb, blk.as<uint32_t>());
-        PTI_CUDA(keys.alloc(padded(n * 8), s), mod);
+        PTI_CUDA(border.alloc(padded(n * 4), s), mod);
+        block_order_kernel<<<grid_n(n), 256, 0, s>>>(blk.as<uint32_t>(), inv.as<uint32_t>(), t->bptr.as<uint64_t>(),
+                                                     nbptr.as<uint64_t>(), n, border.as<uint32_t>());
         PTI_CUDA(order.alloc(padded(n * 4), s), mod);
-        nnz_keys_kernel<<<grid_n(n), 256, 0, s>>>(blk.as<uint32_t>(), inv.as<uint32_t>(),
-                                                  t->einds[mode].as<uint8_t>(), n, keys.as<uint64_t>(),
+        tile_sort_kernel<<<P.ntiles, 256, 0, s>>>(border.as<uint32_t>(), n, blk.as<uint32_t>(),
+                                                  t->binds[mode].as<uint32_t>(), t->einds[mode].as<uint8_t>(), t->sb,
                                                   order.as<uint32_t>());
-        PTI_TRY(rs.alloc(n, s));
-        PTI_TRY(radix_sort_pairs(keys, order, n, (int)bits_for_count(nb) + 8, rs, s));
-        // 3. inside each tile of that order: by output row, stable
-        tile_row_keys_kernel<<<grid_n(n), 256, 0, s>>>(order.as<uint32_t>(), n, blk.as<uint32_t>(),
-                                                       t->binds[mode].as<uint32_t>(), t->einds[mode].as<uint8_t>(),
-                                                       t->sb, keys.as<uint64_t>());
-        PTI_TRY(radix_sort_pairs(keys, order, n, 32 + (int)bits_for_count(P.ntiles), rs, s));
+        border.reset();
         // 4. the nonzeros' encodings in that order
         for (uint32_t k = 0; k < N; ++k) {
             PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
