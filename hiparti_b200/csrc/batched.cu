@@ -743,8 +743,6 @@ __global__ void batch_fill_kernel(float *A, uint64_t n)
     }
 }
 
-int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s);
-
 }  // namespace pti
 
 struct ptiB200Batch {

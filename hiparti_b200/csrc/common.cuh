@@ -50,6 +50,9 @@ namespace pti {
 // Stream used by the synchronous reference entry points: one non-blocking
 // stream per device, created on first use.
 cudaStream_t sync_stream();
+// A second stream per device, for host-to-device copies that overlap work on
+// sync_stream().
+cudaStream_t copy_stream();
 
 // Stream-ordered device allocation from the runtime's default memory pool
 // (cudaMallocAsync).  The pool keeps freed memory for reuse, so repeated calls

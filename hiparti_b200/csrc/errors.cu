@@ -42,6 +42,18 @@ cudaStream_t sync_stream()
     return streams[dev];
 }
 
+cudaStream_t copy_stream()
+{
+    static std::mutex mu;
+    static std::vector<cudaStream_t> streams;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)streams.size() <= dev) streams.resize(dev + 1, nullptr);
+    if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    return streams[dev];
+}
+
 void configure_pool_once()
 {
     static std::mutex mu;

@@ -237,7 +237,8 @@ static bool use_schedule(const ptiB200Tensor *t, uint32_t R)
 }
 
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
-                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s, const float *vals_override)
+                  const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s, const float *vals_override,
+                  cudaEvent_t late)
 {
     const char *mod = "B200 MTTKRP";
     const uint32_t N = t->nmodes;
@@ -266,9 +267,11 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     if (t->nnz == 0) return 0;
     const int G = group_lanes(R);
     if (use_schedule(t, R)) {
-        PTI_TRY(prepare_mode(t, mode, s));
+        PTI_TRY(prepare_mode(t, mode, s, late));
+        if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
         return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s, vals_override);
     }
+    if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
 
     if (!t->hicoo) {
         CooArgs a{};
@@ -418,7 +421,8 @@ int finish_hicoo_layout(ptiB200Tensor *t, cudaStream_t s)
     return 0;
 }
 
-int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s)
+int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s, int first_mode, cudaStream_t s2,
+                 cudaEvent_t late)
 {
     const char *mod = "B200 Upload";
     PTI_CHECK(H && H->nmodes >= 2 && H->nmodes <= (uint32_t)kMaxModes, PTIERR_VALUE_ERROR, mod,
@@ -437,21 +441,33 @@ int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s
     PTI_CHECK(t->nnz == 0 || t->nb > 0, PTIERR_VALUE_ERROR, mod, "HiCOO tensor has nonzeros but no blocks");
     PTI_CHECK(H->values.len >= t->nnz, PTIERR_SHAPE_MISMATCH, mod, "values shorter than nnz");
     PTI_CHECK(t->nb < 0xFFFFFFFFull, PTIERR_VALUE_ERROR, mod, "too many blocks");
-    PTI_CUDA(t->bptr.alloc(padded((t->nb + 1) * 8), s), mod);
-    PTI_CUDA(cudaMemcpyAsync(t->bptr.ptr, H->bptr.data, (t->nb + 1) * 8, cudaMemcpyHostToDevice, s), mod);
-    for (uint32_t m = 0; m < H->nmodes; ++m) {
+    for (uint32_t m = 0; m < H->nmodes; ++m)
         PTI_CHECK(H->binds[m].len >= t->nb && H->einds[m].len >= t->nnz, PTIERR_SHAPE_MISMATCH, mod,
                   "binds/einds shorter than nb/nnz");
+    PTI_CUDA(t->bptr.alloc(padded((t->nb + 1) * 8), s), mod);
+    for (uint32_t m = 0; m < H->nmodes; ++m) {
         PTI_CUDA(t->binds[m].alloc(padded(t->nb * 4), s), mod);
         PTI_CUDA(t->einds[m].alloc(padded(t->nnz), s), mod);
-        if (t->nb)
-            PTI_CUDA(cudaMemcpyAsync(t->binds[m].ptr, H->binds[m].data, t->nb * 4, cudaMemcpyHostToDevice, s), mod);
-        if (t->nnz)
-            PTI_CUDA(cudaMemcpyAsync(t->einds[m].ptr, H->einds[m].data, t->nnz, cudaMemcpyHostToDevice, s), mod);
     }
     PTI_CUDA(t->vals.alloc(padded(t->nnz * 4), s), mod);
+    if (s2) {  // s2 may use the buffers once their stream-ordered allocation is done
+        cudaEvent_t ev;
+        PTI_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), mod);
+        cudaEventRecord(ev, s);
+        cudaStreamWaitEvent(s2, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    PTI_CUDA(cudaMemcpyAsync(t->bptr.ptr, H->bptr.data, (t->nb + 1) * 8, cudaMemcpyHostToDevice, s), mod);
+    for (uint32_t m = 0; m < H->nmodes; ++m) {
+        cudaStream_t cs = s2 && (int)m != first_mode ? s2 : s;
+        if (t->nb)
+            PTI_CUDA(cudaMemcpyAsync(t->binds[m].ptr, H->binds[m].data, t->nb * 4, cudaMemcpyHostToDevice, cs), mod);
+        if (t->nnz)
+            PTI_CUDA(cudaMemcpyAsync(t->einds[m].ptr, H->einds[m].data, t->nnz, cudaMemcpyHostToDevice, cs), mod);
+    }
     if (t->nnz)
-        PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s), mod);
+        PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s2 ? s2 : s), mod);
+    if (s2 && late) PTI_CUDA(cudaEventRecord(late, s2), mod);
     PTI_TRY(ensure_err_word(s));
     if (t->nb) {
         check_bptr_kernel<<<grid_for(t->nb + 1, 256), 256, 0, s>>>(t->bptr.as<uint64_t>(), t->nb, t->nnz,
@@ -484,7 +500,7 @@ int check_mats(uint32_t N, const uint32_t *ndims, ptiMatrix **mats, const char *
 }
 
 int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, ptiIndex mode,
-             cudaStream_t s, const char *mod)
+             cudaStream_t s, const char *mod, cudaEvent_t late = nullptr)
 {
     const uint32_t N = t->nmodes;
     const uint32_t R = mats[mode]->ncols, stride = mats[0]->stride;
@@ -500,7 +516,7 @@ int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, pti
     }
     size_t obytes = (size_t)t->ndims[mode] * stride * 4;
     PTI_CUDA(dout.alloc(padded(obytes), s), mod);
-    PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s));
+    PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s, nullptr, late));
     PTI_CUDA(cudaMemcpyAsync(mats[N]->values, dout.ptr, obytes, cudaMemcpyDeviceToHost, s), mod);
     PTI_TRY(take_device_error(s, mod));
     return 0;
@@ -524,10 +540,21 @@ int mttkrp_host_hicoo(const ptiSparseTensorHiCOO *H, ptiMatrix **mats, const pti
     const char *mod = "B200 HiSpTns MTTKRP";
     PTI_CHECK(H && mode < H->nmodes, PTIERR_VALUE_ERROR, mod, "bad tensor or mode");
     PTI_TRY(check_mats(H->nmodes, H->ndims, mats, mod));
-    cudaStream_t s = sync_stream();
-    ptiB200Tensor t;
-    PTI_TRY(upload_hicoo(&t, H, s));
-    return run_host(&t, mats, mats_order, mode, s, mod);
+    // The arrays mode `mode`'s schedule starts from (block pointers, the
+    // mode's coordinates and offsets) are copied first on s; the rest follows
+    // on a second stream while the schedule is being built.
+    cudaStream_t s = sync_stream(), s2 = copy_stream();
+    cudaEvent_t late = nullptr;
+    PTI_CUDA(cudaEventCreateWithFlags(&late, cudaEventDisableTiming), mod);
+    int r;
+    {
+        ptiB200Tensor t;
+        r = upload_hicoo(&t, H, s, (int)mode, s2, late);
+        if (r == 0) r = run_host(&t, mats, mats_order, mode, s, mod, late);
+        cudaStreamWaitEvent(s, late, 0);  // the tensor is released on s only after the second stream's copies
+    }
+    cudaEventDestroy(late);
+    return r;
 }
 
 }  // namespace pti

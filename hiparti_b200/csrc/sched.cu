@@ -628,7 +628,7 @@ static unsigned grid_n(uint64_t n)
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 32));
 }
 
-int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
+int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, cudaEvent_t late)
 {
     const char *mod = "B200 Prepare";
     PTI_CHECK(mode < t->nmodes, PTIERR_VALUE_ERROR, mod, "mode out of range");
@@ -693,13 +693,7 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
         PTI_CUDA(cudaMemcpyAsync(nbptr.as<uint64_t>() + nb, tmp.as<uint64_t>() + (nb + kScanTile - 1) / kScanTile,
                                  8, cudaMemcpyDeviceToDevice, s), mod);
     }
-    for (uint32_t k = 0; k < N; ++k) {
-        PTI_CUDA(P.binds[k].alloc(padded(nb * 4), s), mod);
-        gather_kernel<uint32_t><<<grid_n(nb), 256, 0, s>>>(t->binds[k].as<uint32_t>(), bperm.as<uint32_t>(), nb,
-                                                           P.binds[k].as<uint32_t>());
-    }
     bsize.reset();
-    bperm.reset();
     P.nb = nb;
     P.ntiles = (uint32_t)((n + kHiTile - 1) / kHiTile);
     PTI_CUDA(P.tile_block.alloc(padded(((size_t)P.ntiles + 1) * 4), s), mod);
@@ -719,7 +713,15 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s)
                                                   t->binds[mode].as<uint32_t>(), t->einds[mode].as<uint8_t>(), t->sb,
                                                   order.as<uint32_t>());
         border.reset();
-        // 4. the nonzeros' encodings in that order
+        // 4. everything up to here read only bptr and the output mode's arrays;
+        // the gathers below read every array
+        if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
+        for (uint32_t k = 0; k < N; ++k) {
+            PTI_CUDA(P.binds[k].alloc(padded(nb * 4), s), mod);
+            gather_kernel<uint32_t><<<grid_n(nb), 256, 0, s>>>(t->binds[k].as<uint32_t>(), bperm.as<uint32_t>(), nb,
+                                                               P.binds[k].as<uint32_t>());
+        }
+        bperm.reset();
         for (uint32_t k = 0; k < N; ++k) {
             PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
             gather_kernel<uint8_t><<<grid_n(n), 256, 0, s>>>(t->einds[k].as<uint8_t>(), order.as<uint32_t>(), n,

@@ -70,15 +70,22 @@ struct ptiB200Tensor {
 namespace pti {
 
 int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
-int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s);
+// With s2, the arrays that mode first_mode's schedule does not need first
+// (the other modes' coordinates and offsets, the values) are copied on s2, and
+// `late` is recorded on s2 after them.
+int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s, int first_mode = -1,
+                 cudaStream_t s2 = nullptr, cudaEvent_t late = nullptr);
 
 // MTTKRP launchers; factors are device pointers (element type ft), out is FP32.
 // vals_override (optional): nnz values in the tensor's input order that replace
 // its own values (COO tensors only).
+// late (optional): an event after which all of the tensor's arrays are on
+// the device; the schedule build and the kernel wait for it only where they
+// need the arrays it covers.
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                   const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
-                  const float *vals_override = nullptr);
-int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s);
+                  const float *vals_override = nullptr, cudaEvent_t late = nullptr);
+int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, cudaEvent_t late = nullptr);
 
 // Host-struct MTTKRP used by the reference entry points.
 int mttkrp_host_coo(const ptiSparseTensor *X, ptiMatrix **mats, const ptiIndex *mats_order,
