@@ -345,6 +345,7 @@ def run_batched(args):
     from hiparti_b200 import DeviceTensor
     from hiparti_b200.batched import Batch, stride_for
     dev = torch.device("cuda", torch.cuda.current_device())
+    iters = args.batched_iters
     tensors, ranks = make_c5(dev, SEED + 21)
     total_nnz = sum(int(v.numel()) for _, _, v in tensors)
     bt = Batch(tensors, ranks, tune=True)
@@ -360,7 +361,7 @@ def run_batched(args):
             fs.append(a)
         init.append(fs)
     out = {"workload": f"C5 batched CPD-ALS: {C5_TENSORS} 3-D tensors, dims U{{50..5000}}, nnz log-U[1e3,1e6] "
-                       f"(total {total_nnz}), U(0,1) values, ranks from {{8,16,32}}, {C5_ITERS} iterations",
+                       f"(total {total_nnz}), U(0,1) values, ranks from {{8,16,32}}, {iters} iterations",
            "total_nnz": total_nnz, "sb_bits": info["sb_bits"], "cols_per_lane_bf16": info["cols_per_lane"],
            "tasks_per_iter": info["ntasks"], "tune_s": round(info["tune_ms"] / 1e3, 3),
            "setup_s": round(info["setup_ms"] / 1e3, 3)}
@@ -369,7 +370,7 @@ def run_batched(args):
         facs = [[a.clone() for a in fs] for fs in init]
         bt.cpd_als(facs, 2, precision=prec, fp32_sweeps=1)  # warm-up
         facs = [[a.clone() for a in fs] for fs in init]
-        _, f, ms = bt.cpd_als(facs, C5_ITERS, precision=prec, fp32_sweeps=2 if prec == "bf16" else C5_ITERS)
+        _, f, ms = bt.cpd_als(facs, iters, precision=prec, fp32_sweeps=2 if prec == "bf16" else iters)
         fits[prec] = f[:, -1]
         out[f"ms_per_iter_{prec}"] = round(ms, 4)
         # MTTKRP work of one iteration: every nonzero of every tensor, 3 modes
@@ -385,9 +386,9 @@ def run_batched(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for t, fs, R in zip(dts, facs, ranks):
-            t.cpd_als(fs, C5_ITERS, rank=R)
+            t.cpd_als(fs, iters, rank=R)
         torch.cuda.synchronize()
-        out["ms_per_iter_fp32_tensor_by_tensor"] = round((time.perf_counter() - t0) * 1e3 / C5_ITERS, 3)
+        out["ms_per_iter_fp32_tensor_by_tensor"] = round((time.perf_counter() - t0) * 1e3 / iters, 3)
         for t in dts:
             t.free()
     if args.batched_oracle > 0:
@@ -402,7 +403,7 @@ def run_batched(args):
             dims, inds, vals = tensors[b]
             R = ranks[b]
             o = orc.cpd_als(list(dims), [i.cpu().numpy().astype(np.uint32) for i in inds], vals.cpu().numpy(), R,
-                            C5_ITERS, [a[:, :R].cpu().numpy() for a in init[b]])
+                            iters, [a[:, :R].cpu().numpy() for a in init[b]])
             d32.append(abs(fits["fp32"][b] - o["fit"]))
             d16.append(abs(fits["bf16"][b] - o["fit"]))
         out["oracle_tensors"] = int(len(pick))
@@ -644,6 +645,9 @@ def main():
     ap.add_argument("--no-cpd", action="store_true", help="skip the CPD-ALS (C3) block")
     ap.add_argument("--no-gradcp", action="store_true", help="skip the gradient-CP (C4) block")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched CPD-ALS (C5) block")
+    ap.add_argument("--batched-iters", type=int, default=C5_ITERS)
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched"], default=None,
+                    help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
                     help="C5 tensors (spread over the size range) checked against the FP64 oracle")
     ap.add_argument("--batched-sequential", type=int, default=1,
@@ -666,6 +670,12 @@ def main():
 
     from hiparti_b200 import build
     build.build()
+    if args.only:
+        import torch
+        torch.cuda.set_device(0)
+        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched}[args.only]
+        print(json.dumps({"only": args.only, **block(args)}), flush=True)
+        return
     rank, world, _ = dist_setup(args.gpus)
     res = run_ours_mttkrp(args, rank, world)
     if rank == 0:
