@@ -123,34 +123,18 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus):
-    import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
-        torch.cuda.set_device(0)
-    return rank, world, local
+    from hiparti_b200 import replicas
+    return replicas.setup("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from hiparti_b200 import replicas
+    replicas.barrier(world)
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from hiparti_b200 import replicas
+    return replicas.max_over_ranks(x, world)
 
 
 def make_c2(device, seed, nnz=C2_NNZ):
@@ -694,9 +678,8 @@ def main():
             torch.cuda.empty_cache()
             res["batched"] = run_batched(args)
         print(json.dumps(res), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from hiparti_b200 import replicas
+    replicas.shutdown(world)
 
 
 if __name__ == "__main__":
