@@ -50,6 +50,27 @@ def hicoo_bytes(nnz, nb, dims, R, N, fsize=4):
     return nnz * (N + 4) + nb * (8 + 4 * N) + fsize * R * sum(dims)
 
 
+def factor_match_score(lam_a, facs_a, lam_b, facs_b):
+    """Factor match score of two CP models (Acar et al.): the components are
+    paired by the best assignment of the product over modes of the absolute
+    column cosines; each pair scores that product times
+    1 - |lambda_a - lambda_b| / max(lambda_a, lambda_b); the score is the mean
+    over components (1 = the same model)."""
+    from scipy.optimize import linear_sum_assignment
+    R = len(lam_a)
+    sim = np.ones((R, R))
+    for A, B in zip(facs_a, facs_b):
+        A = np.asarray(A, np.float64)[:, :R]
+        B = np.asarray(B, np.float64)[:, :R]
+        na = np.linalg.norm(A, axis=0)
+        nb = np.linalg.norm(B, axis=0)
+        sim *= np.abs(A.T @ B) / np.maximum(np.outer(na, nb), 1e-300)
+    rows, cols = linear_sum_assignment(-sim)
+    la, lb = np.abs(np.asarray(lam_a, np.float64)), np.abs(np.asarray(lam_b, np.float64))
+    pen = 1.0 - np.abs(la[rows] - lb[cols]) / np.maximum(np.maximum(la[rows], lb[cols]), 1e-300)
+    return float(np.mean(sim[rows, cols] * pen))
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -218,7 +239,7 @@ def run_cpd(args):
                               fp32_sweeps=args.fp32_sweeps if prec == "bf16" else args.cpd_iters)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        results[prec] = (dt / args.cpd_iters, fits[-1])
+        results[prec] = (dt / args.cpd_iters, fits[-1], lam.cpu().numpy(), [f[:, :C3_R].cpu().numpy() for f in fac])
         out[f"s_per_iter_{prec}"] = round(dt / args.cpd_iters, 6)
         out[f"fit_{prec}"] = fits[-1]
     out["speedup_bf16_vs_fp32"] = round(results["fp32"][0] / results["bf16"][0], 3)
@@ -233,6 +254,9 @@ def run_cpd(args):
         out["oracle_s"] = round(time.perf_counter() - t0, 1)
         out["fit_diff_fp32"] = abs(results["fp32"][1] - o["fit"])
         out["fit_diff_bf16"] = abs(results["bf16"][1] - o["fit"])
+        for prec in ["fp32", "bf16"]:
+            out[f"fms_{prec}_vs_oracle"] = round(factor_match_score(results[prec][2], results[prec][3],
+                                                                    o["lambda_"], o["factors"]), 6)
     coo.free()
     if t is not coo:
         t.free()
@@ -349,13 +373,14 @@ def run_batched(args):
            "total_nnz": total_nnz, "sb_bits": info["sb_bits"], "cols_per_lane_bf16": info["cols_per_lane"],
            "tasks_per_iter": info["ntasks"], "tune_s": round(info["tune_ms"] / 1e3, 3),
            "setup_s": round(info["setup_ms"] / 1e3, 3)}
-    fits = {}
+    fits, models = {}, {}
     for prec in ["fp32", "bf16"]:
         facs = [[a.clone() for a in fs] for fs in init]
         bt.cpd_als(facs, 2, precision=prec, fp32_sweeps=1)  # warm-up
         facs = [[a.clone() for a in fs] for fs in init]
-        _, f, ms = bt.cpd_als(facs, iters, precision=prec, fp32_sweeps=2 if prec == "bf16" else iters)
+        lams, f, ms = bt.cpd_als(facs, iters, precision=prec, fp32_sweeps=2 if prec == "bf16" else iters)
         fits[prec] = f[:, -1]
+        models[prec] = (lams, facs)
         out[f"ms_per_iter_{prec}"] = round(ms, 4)
         # MTTKRP work of one iteration: every nonzero of every tensor, 3 modes
         out[f"gnnz_modes_per_s_{prec}"] = round(3 * total_nnz / (ms * 1e-3) / 1e9, 2)
@@ -382,7 +407,7 @@ def run_batched(args):
         order = np.argsort([int(v.numel()) for _, _, v in tensors])
         pick = order[np.linspace(0, len(order) - 1, min(args.batched_oracle, len(order))).round().astype(int)]
         t0 = time.perf_counter()
-        d32, d16 = [], []
+        d32, d16, f32s, f16s = [], [], [], []
         for b in pick:
             dims, inds, vals = tensors[b]
             R = ranks[b]
@@ -390,10 +415,16 @@ def run_batched(args):
                             iters, [a[:, :R].cpu().numpy() for a in init[b]])
             d32.append(abs(fits["fp32"][b] - o["fit"]))
             d16.append(abs(fits["bf16"][b] - o["fit"]))
+            for prec, acc in (("fp32", f32s), ("bf16", f16s)):
+                lams, facs = models[prec]
+                acc.append(factor_match_score(lams[b].cpu().numpy(), [x[:, :R].cpu().numpy() for x in facs[b]],
+                                              o["lambda_"], o["factors"]))
         out["oracle_tensors"] = int(len(pick))
         out["oracle_s"] = round(time.perf_counter() - t0, 1)
         out["max_fit_diff_fp32"] = float(max(d32))
         out["max_fit_diff_bf16"] = float(max(d16))
+        out["min_fms_fp32_vs_oracle"] = round(float(min(f32s)), 6)
+        out["min_fms_bf16_vs_oracle"] = round(float(min(f16s)), 6)
     out["fit_bf16_min_max"] = [float(fits["bf16"].min()), float(fits["bf16"].max())]
     return out
 
