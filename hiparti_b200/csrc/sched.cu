@@ -747,7 +747,8 @@ template <int G, int CPL, int U, class FT, int NIN>
 static int launch_coo(const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = (size_t)kTile * Rec<NIN>::words * 4 + (size_t)kSchedThreads * CPL * 4;
-    auto k = coo_sched_kernel<G, CPL, U, 4, FT, NIN>;
+    constexpr int UU = NIN == 3 && U > 2 ? 2 : U;  // 4-D records hold more registers per nonzero
+    auto k = coo_sched_kernel<G, CPL, UU, 4, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a, recs);
