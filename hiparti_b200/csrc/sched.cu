@@ -62,33 +62,37 @@ struct Rec {
     static constexpr int words = ((NIN + 2 + 3) / 4) * 4;
 };
 
-// Columns of one operand row held by a lane: 4 (one float4 of FP32) or 8 (one
-// 16-byte load of BF16).
+// Columns of one operand row held by a lane: CPL consecutive columns, loaded
+// with 8- or 16-byte loads (4 FP32 columns = one 16-byte load, 8 FP32 = two,
+// 8 BF16 = one, 4 BF16 = one 8-byte load).
 template <int CPL, class FT>
 struct RowPart {
-    uint4 raw;
+    static constexpr int kWords = CPL * (int)sizeof(FT) / 4;
+    static_assert(kWords == 2 || kWords % 4 == 0, "8- or 16-byte loads");
+    uint32_t w[kWords];
     __device__ __forceinline__ void load(const FT *row, uint32_t col)
     {
-        if constexpr (CPL == 4 && sizeof(FT) == 4) {
-            const float4 f = __ldg(reinterpret_cast<const float4 *>(row + col));
-            raw = make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z), __float_as_uint(f.w));
-        } else if constexpr (CPL == 8) {
-            raw = __ldg(reinterpret_cast<const uint4 *>(row + col));
+        const FT *p = row + col;
+        if constexpr (kWords == 2) {
+            const uint2 r = __ldg(reinterpret_cast<const uint2 *>(p));
+            w[0] = r.x;
+            w[1] = r.y;
         } else {
-            const uint2 r = __ldg(reinterpret_cast<const uint2 *>(row + col));
-            raw = make_uint4(r.x, r.y, 0u, 0u);
+#pragma unroll
+            for (int q = 0; q < kWords / 4; ++q) {
+                const uint4 r = __ldg(reinterpret_cast<const uint4 *>(p) + q);
+                w[4 * q] = r.x;
+                w[4 * q + 1] = r.y;
+                w[4 * q + 2] = r.z;
+                w[4 * q + 3] = r.w;
+            }
         }
     }
     // 32-bit word i of the loaded columns
-    __device__ __forceinline__ uint32_t word(int i) const
-    {
-        const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
-        return w[i];
-    }
+    __device__ __forceinline__ uint32_t word(int i) const { return w[i]; }
     // column c (0 <= c < CPL) as FP32
     __device__ __forceinline__ float at(int c) const
     {
-        const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
         if constexpr (sizeof(FT) == 4) {
             return __uint_as_float(w[c]);
         } else {
