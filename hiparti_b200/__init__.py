@@ -6,6 +6,7 @@ This package is the Python face of that library: cffi bindings generated from
 the header, numpy-backed host tensors, and torch-facing device tensors.
 """
 from ._ffi import PtiError, ffi, last_error, lib
-from .api import COOTensor, DeviceTensor, HiCOOTensor
+from .api import COOTensor, DeviceTensor, HiCOOTensor, dump_kruskal, load_cpd_checkpoint
 
-__all__ = ["COOTensor", "HiCOOTensor", "DeviceTensor", "PtiError", "ffi", "lib", "last_error"]
+__all__ = ["COOTensor", "HiCOOTensor", "DeviceTensor", "PtiError", "ffi", "lib", "last_error",
+           "load_cpd_checkpoint", "dump_kruskal"]

@@ -360,11 +360,16 @@ class DeviceTensor:
                                         mode, ffi.cast("float *", out.data_ptr()), stream), "ptiB200MTTKRPValues")
         return out
 
-    def cpd_als(self, factors, niters, tol=0.0, precision="fp32", fp32_sweeps=1, rank=None):
+    def cpd_als(self, factors, niters, tol=0.0, precision="fp32", fp32_sweeps=1, rank=None,
+                checkpoint=None, checkpoint_every=0, resume=False):
         """CPD-ALS on the device (ptiB200CpdAls).  factors: list of float32 CUDA
         tensors (I_k, stride) holding the initial factors; updated in place.
         precision "bf16" makes the MTTKRP gathers read BF16 copies for all but
-        the last fp32_sweeps iterations.  Returns (lambda, fits)."""
+        the last fp32_sweeps iterations.  checkpoint: a file that receives the
+        loop state after every checkpoint_every iterations (0: only the last);
+        resume=True continues from it when it exists
+        (ptiB200CpdAlsCheckpoint).  Returns (lambda, fits), fits counting the
+        restored iterations too."""
         import torch
         stride = factors[0].shape[1]
         R = stride if rank is None else int(rank)
@@ -374,8 +379,11 @@ class DeviceTensor:
         fp = ffi.new("float *[]", [ffi.cast("float *", f.data_ptr()) for f in factors])
         stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
         prec = {"fp32": _F32, "bf16": _BF16}[precision]
-        check(lib().ptiB200CpdAls(self._h, R, niters, tol, prec, fp32_sweeps, fp, stride,
-                                  ffi.cast("float *", lam.data_ptr()), fits, done, stream), "ptiB200CpdAls")
+        path = ffi.NULL if checkpoint is None else str(checkpoint).encode()
+        check(lib().ptiB200CpdAlsCheckpoint(self._h, R, niters, tol, prec, fp32_sweeps, fp, stride,
+                                            ffi.cast("float *", lam.data_ptr()), fits, done, path,
+                                            int(checkpoint_every), int(bool(resume)), stream),
+              "ptiB200CpdAlsCheckpoint")
         return lam, [fits[i] for i in range(done[0])]
 
     def free(self):
@@ -388,3 +396,58 @@ class DeviceTensor:
             self.free()
         except Exception:
             pass
+
+
+# ----------------------------------------------------------------------------
+# CPD results on the host: checkpoints and the reference's text dump
+# ----------------------------------------------------------------------------
+def load_cpd_checkpoint(path):
+    """Reads a CPD checkpoint (ptiB200LoadCpdCheckpoint): the result the ALS
+    loop returns after the stored iterations.  Returns a dict with iters, fit,
+    lambda_ (R,) and factors (list of (I_k, R) float32 arrays)."""
+    k = ffi.new("ptiKruskalTensor *")
+    it = ffi.new("ptiIndex *")
+    check(lib().ptiB200LoadCpdCheckpoint(k, it, str(path).encode()), "ptiB200LoadCpdCheckpoint")
+    try:
+        R = k.rank
+        lam = np.frombuffer(ffi.buffer(getattr(k, "lambda"), 4 * R), np.float32).copy()
+        facs = []
+        for m in range(k.nmodes):
+            f = k.factors[m]
+            a = np.frombuffer(ffi.buffer(f.values, 4 * f.nrows * f.stride), np.float32)
+            facs.append(a.reshape(f.nrows, f.stride)[:, :R].copy())
+        return dict(iters=int(it[0]), fit=float(k.fit), lambda_=lam, factors=facs)
+    finally:
+        lib().ptiFreeKruskalTensor(k)
+
+
+def dump_kruskal(path, lambda_, factors, fit=0.0):
+    """Writes a Kruskal tensor as text in the reference's format
+    (ptiDumpKruskalTensor, src/ktensor/dump.c:23-55)."""
+    lam = np.ascontiguousarray(lambda_, np.float32)
+    facs = [np.ascontiguousarray(f, np.float32) for f in factors]
+    R, N = lam.size, len(facs)
+    dims = ffi.new("ptiIndex[]", [f.shape[0] for f in facs])
+    k = ffi.new("ptiKruskalTensor *")
+    L = lib()
+    check(L.ptiNewKruskalTensor(k, N, dims, R), "ptiNewKruskalTensor")
+    mats = ffi.new("ptiMatrix *[]", N + 1)
+    structs = [ffi.new("ptiMatrix *") for _ in range(N)]
+    try:
+        for m, f in enumerate(facs):
+            check(L.ptiNewMatrix(structs[m], f.shape[0], R), "ptiNewMatrix")
+            st = structs[m].stride
+            buf = np.frombuffer(ffi.buffer(structs[m].values, 4 * f.shape[0] * st), np.float32)
+            buf.reshape(f.shape[0], st)[:, :R] = f[:, :R]
+            mats[m] = structs[m]
+        ffi.memmove(getattr(k, "lambda"), lam.tobytes(), 4 * R)
+        k.fit = float(fit)
+        k.factors = mats
+        with open(path, "wb") as fh:
+            check(L.ptiDumpKruskalTensor(k, fh), "ptiDumpKruskalTensor")
+    finally:
+        k.factors = ffi.NULL
+        for sm in structs:
+            if sm.values != ffi.NULL:
+                L.ptiFreeMatrix(sm)
+        L.ptiFreeKruskalTensor(k)

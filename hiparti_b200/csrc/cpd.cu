@@ -20,6 +20,7 @@
 // ssyrk_ call does not write, so its printed fit is not the model's fit.)
 #include <cuda_bf16.h>
 
+#include "checkpoint.cuh"
 #include "spd.cuh"
 #include "tensor.cuh"
 
@@ -331,16 +332,22 @@ struct CpdOptions {
     double tol = 0.0;
     int precision = PTI_B200_F32;  // factors read by MTTKRP: F32 or BF16
     uint32_t fp32_sweeps = 1;      // closing iterations with FP32 factors (mixed mode)
+    const char *ckpt_path = nullptr;  // checkpoint file (nullptr: none)
+    uint32_t ckpt_every = 0;          // write after every ckpt_every iterations; always after the last
+    bool resume = false;              // continue from ckpt_path when the file exists
 };
 
 struct CpdResult {
     std::vector<double> fits;
     uint32_t iters = 0;
-    int solver_flags = 0;  // OR of gram_inverse flags seen
+    uint32_t resumed_from = 0;  // iterations restored from a checkpoint
+    int solver_flags = 0;       // OR of gram_inverse flags seen
 };
 
 // A[m] (device, I_m x stride FP32) hold the initial factors on entry and the
-// result on exit; lambda (device, R floats) receives the weights.
+// result on exit; lambda (device, R floats) receives the weights.  With a
+// checkpoint file and `resume`, the loop state stored there replaces the
+// initial factors and the loop continues after its last iteration.
 int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda, const CpdOptions &opt,
                CpdResult &res, cudaStream_t s)
 {
@@ -371,6 +378,34 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
         for (uint32_t m = 0; m < N; ++m)
             PTI_CUDA(Ab[m].alloc(padded((size_t)t->ndims[m] * stride * 2), s), mod);
 
+    // Resume: the stored loop state replaces the initial factors.  The row
+    // pad columns are zeroed, as the solves leave them.
+    CkptState st;
+    bool have_ckpt = false;
+    if (opt.resume && opt.ckpt_path) {
+        bool missing = false;
+        PTI_TRY(ckpt_read(opt.ckpt_path, st, &missing));
+        have_ckpt = !missing;
+    }
+    if (have_ckpt) {
+        bool same = st.nmodes == N && st.rank == R && st.nnz == t->nnz;
+        for (uint32_t m = 0; same && m < N; ++m) same = st.ndims[m] == t->ndims[m];
+        PTI_CHECK(same, PTIERR_SHAPE_MISMATCH, mod, "checkpoint is of another tensor shape or rank");
+        PTI_CHECK(st.iters <= opt.niters, PTIERR_VALUE_ERROR, mod, "checkpoint holds more iterations than niters");
+        for (uint32_t m = 0; m < N; ++m) {
+            if (!t->ndims[m]) continue;
+            PTI_CUDA(cudaMemsetAsync(A[m], 0, (size_t)t->ndims[m] * stride * 4, s), mod);
+            PTI_CUDA(cudaMemcpy2DAsync(A[m], (size_t)stride * 4, st.factors[m].data(), (size_t)R * 4, (size_t)R * 4,
+                                       t->ndims[m], cudaMemcpyHostToDevice, s),
+                     mod);
+        }
+        PTI_CUDA(cudaMemcpyAsync(lambda, st.lambda.data(), (size_t)R * 4, cudaMemcpyHostToDevice, s), mod);
+        if (st.iters)
+            PTI_CUDA(cudaMemcpyAsync(fits, st.fits.data(), (size_t)st.iters * 8, cudaMemcpyHostToDevice, s), mod);
+    }
+    CkptWriter writer;
+    if (opt.ckpt_path) PTI_TRY(writer.init(opt.ckpt_path, N, t->ndims.data(), t->nnz, R, opt.niters));
+
     const size_t gram_smem = (size_t)(RR + 32 * R) * 8;
     const size_t solve_smem = (size_t)RR * 8 + (size_t)R * 12;
     PTI_CUDA(cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem), mod);
@@ -389,12 +424,23 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
     if (t->nnz) sumsq_kernel<<<rows_grid(t->nnz, 256), 256, 0, s>>>(t->vals.as<float>(), t->nnz, normX2);
     PTI_CUDA(cudaGetLastError(), mod);
 
+    if (have_ckpt) {
+        // The sum of squares tells a different tensor of the same shape.
+        double nx = 0.0;
+        PTI_CUDA(cudaMemcpyAsync(&nx, normX2, 8, cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+        PTI_CHECK(std::fabs(nx - st.normX2) <= 1e-6 * std::max(std::fabs(nx), std::fabs(st.normX2)),
+                  PTIERR_VALUE_ERROR, mod, "checkpoint is of another tensor (sum of squared values differs)");
+    }
+
     std::vector<uint32_t> order(N);
     std::vector<const void *> fptr(N);
     res.fits.clear();
-    double oldfit = 0.0;
-    uint32_t it = 0;
-    for (; it < opt.niters; ++it) {
+    res.resumed_from = have_ckpt ? st.iters : 0;
+    double oldfit = have_ckpt && st.iters ? st.fits[st.iters - 1] : 0.0;
+    bool converged = have_ckpt && (st.flags & kCkptConverged) && opt.tol > 0.0;
+    uint32_t it = have_ckpt ? st.iters : 0;
+    for (; it < opt.niters && !converged; ++it) {
         const bool use_bf16 = mixed && it + opt.fp32_sweeps < opt.niters;
         for (uint32_t k = 0; k < N; ++k)
             fptr[k] = use_bf16 ? (const void *)Ab[k].ptr : (const void *)A[k];
@@ -428,12 +474,12 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
             PTI_CUDA(cudaMemcpyAsync(&fit, fits + it, 8, cudaMemcpyDeviceToHost, s), mod);
             PTI_CUDA(cudaStreamSynchronize(s), mod);
             // cpd.c:144: stop when the fit changes by less than tol
-            if (it > 0 && std::fabs(fit - oldfit) < opt.tol) {
-                ++it;
-                break;
-            }
+            converged = it > 0 && std::fabs(fit - oldfit) < opt.tol;
             oldfit = fit;
         }
+        if (opt.ckpt_path &&
+            (converged || it + 1 == opt.niters || (opt.ckpt_every && (it + 1) % opt.ckpt_every == 0)))
+            PTI_TRY(writer.save(A, stride, lambda, fits, normX2, it + 1, converged, s));
     }
     res.iters = it;
     // GetFinalLambda (matrix.c:556-572)
@@ -451,6 +497,7 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
     PTI_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s), mod);
     PTI_CUDA(cudaStreamSynchronize(s), mod);
     res.solver_flags = hflag;
+    PTI_TRY(writer.finish());
     return 0;
 }
 
@@ -600,14 +647,27 @@ int ptiB200CpdAls(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, 
                   float *const *dev_factors, ptiIndex stride, float *dev_lambda, double *fits, ptiIndex *iters_done,
                   void *stream)
 {
+    return ptiB200CpdAlsCheckpoint(t, rank, niters, tol, precision, fp32_sweeps, dev_factors, stride, dev_lambda,
+                                   fits, iters_done, nullptr, 0, 0, stream);
+}
+
+int ptiB200CpdAlsCheckpoint(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, int precision,
+                            ptiIndex fp32_sweeps, float *const *dev_factors, ptiIndex stride, float *dev_lambda,
+                            double *fits, ptiIndex *iters_done, const char *ckpt_path, ptiIndex ckpt_every,
+                            int resume, void *stream)
+{
     using namespace pti;
     PTI_CHECK(t && dev_factors && dev_lambda, PTIERR_VALUE_ERROR, "B200 CPD-ALS", "null argument");
+    PTI_CHECK(!resume || ckpt_path, PTIERR_VALUE_ERROR, "B200 CPD-ALS", "resume needs a checkpoint path");
     CpdOptions opt;
     opt.R = rank;
     opt.niters = niters;
     opt.tol = tol;
     opt.precision = precision;
     opt.fp32_sweeps = fp32_sweeps;
+    opt.ckpt_path = ckpt_path && *ckpt_path ? ckpt_path : nullptr;
+    opt.ckpt_every = ckpt_every;
+    opt.resume = resume != 0;
     CpdResult res;
     PTI_TRY(cpd_device(t, dev_factors, stride, dev_lambda, opt, res, static_cast<cudaStream_t>(stream)));
     if (fits)

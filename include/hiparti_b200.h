@@ -167,6 +167,15 @@ void ptiFreeRankKruskalTensor(ptiRankKruskalTensor *ktsr);
 int  ptiNewRankMatrix(ptiRankMatrix *mtx, ptiIndex const nrows, ptiElementIndex const ncols);
 void ptiFreeRankMatrix(ptiRankMatrix *mtx);
 
+/* Text dumps in the reference's format: include/includes/matrices.h:35,74
+ * (src/matrix/dump.c:33-75: "<rows> x <cols> matrix", then rows of "%.2f\t")
+ * and include/includes/ktensors.h:26,46 (src/ktensor/dump.c:23-88: sizes,
+ * "fit: ", "lambda:", "Factor matrices:").  Host only. */
+int ptiDumpMatrix(ptiMatrix *mtx, FILE *fp);
+int ptiDumpRankMatrix(ptiRankMatrix *mtx, FILE *fp);
+int ptiDumpKruskalTensor(ptiKruskalTensor *ktsr, FILE *fp);
+int ptiDumpRankKruskalTensor(ptiRankKruskalTensor *ktsr, FILE *fp);
+
 /* include/includes/sptensors.h:104-119 */
 int  ptiNewSparseTensorHiCOO(ptiSparseTensorHiCOO *hitsr, const ptiIndex nmodes, const ptiIndex ndims[],
                              const ptiNnzIndex nnz, const ptiElementIndex sb_bits,
@@ -328,6 +337,29 @@ int ptiB200MTTKRPHiCOONoAlloc(ptiIndex nmodes, const ptiIndex *ndims, ptiNnzInde
 int ptiB200CpdAls(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, int precision,
                   ptiIndex fp32_sweeps, float * const *dev_factors, ptiIndex stride, float *dev_lambda,
                   double *fits, ptiIndex *iters_done, void *stream);
+
+/* ptiB200CpdAls with checkpoints (the reference has none; its CPD writes its
+ * result only as text, src/ktensor/dump.c:23-55).  ckpt_path (may be NULL:
+ * none) receives the ALS loop state -- factors, weights and every fit so far
+ * -- after every ckpt_every iterations (0: only the last) and after the last
+ * iteration; the file is written from a background thread, as <path>.tmp
+ * renamed over <path>.  With resume != 0 and an existing file, that state
+ * replaces the initial factors and the loop continues after its last
+ * iteration (a run that had converged under tol > 0 is not iterated further);
+ * fits and iters_done then count the restored iterations too.  A checkpoint of
+ * another shape, rank or tensor, or of more than niters iterations, is
+ * rejected; a missing file starts from the initial factors. */
+int ptiB200CpdAlsCheckpoint(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, double tol, int precision,
+                            ptiIndex fp32_sweeps, float * const *dev_factors, ptiIndex stride,
+                            float *dev_lambda, double *fits, ptiIndex *iters_done,
+                            const char *ckpt_path, ptiIndex ckpt_every, int resume, void *stream);
+
+/* Reads a checkpoint written by ptiB200CpdAlsCheckpoint into a host Kruskal
+ * tensor, finished as the ALS loop finishes its result (columns scaled to unit
+ * 2-norm, weights multiplied by the norms, src/matrix/matrix.c:556-572); fit is
+ * the last fit.  ktsr is created here (release it with ptiFreeKruskalTensor);
+ * iters_done (may be NULL) receives the stored iteration count.  Host only. */
+int ptiB200LoadCpdCheckpoint(ptiKruskalTensor *ktsr, ptiIndex *iters_done, const char *path);
 
 /* Batched CPD-ALS of many independent 3-D tensors of uneven size and rank (no
  * counterpart in the reference, whose CPD entry points factor one tensor per
