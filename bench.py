@@ -317,6 +317,88 @@ def run_gradcp(args):
             "ms_per_gradient": round(ms, 3), "loss": float(loss.item())}
 
 
+INGEST_NNZ = 10_000_000
+INGEST_REF_NNZ = 1_000_000
+
+
+def write_tns_fixed(path, dims, inds, vals_u6):
+    """Writes a .tns file with fixed-width fields: 1-based indices zero-padded
+    to the widest mode size and values "0.dddddd" (vals_u6 = int(v * 1e6)).
+    fscanf reads leading zeros like any other digits."""
+    import numpy as np
+    cols = []
+    for d, ix in zip(dims, inds):
+        w = len(str(d))
+        pw = 10 ** np.arange(w - 1, -1, -1, dtype=np.int64)
+        cols.append((((ix.astype(np.int64) + 1)[:, None] // pw) % 10 + 48).astype(np.uint8))
+        cols.append(np.full((ix.size, 1), 32, np.uint8))
+    pw = 10 ** np.arange(5, -1, -1, dtype=np.int64)
+    cols.append(np.tile(np.frombuffer(b"0.", np.uint8), (vals_u6.size, 1)))
+    cols.append(((vals_u6.astype(np.int64)[:, None] // pw) % 10 + 48).astype(np.uint8))
+    cols.append(np.full((vals_u6.size, 1), 10, np.uint8))
+    body = np.concatenate(cols, axis=1)
+    with open(path, "wb") as f:
+        f.write(f"{len(dims)}\n{' '.join(map(str, dims))}\n".encode())
+        f.write(body.tobytes())
+
+
+def run_ingest(args):
+    """GPU tensor ingest: a 10M-nonzero .tns file with the C2 construction's
+    dims and Zipf(1.1) coordinates (fixed-width text, U(0,1) values with six
+    decimals) loaded by ptiB200LoadSparseTensor from the page cache into device
+    memory; the reference's fscanf loader (oracle/_ref, compiled from
+    src/sptensor/load.c) timed on a 1M-nonzero file of the same construction."""
+    import tempfile
+    import time
+    import numpy as np
+    import torch
+    from hiparti_b200 import DeviceTensor
+    from hiparti_b200.synth import coords_torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    out = {"workload": f"ingest: .tns text, 3-D {C2_DIMS[0]}x{C2_DIMS[1]}x{C2_DIMS[2]}, Zipf(1.1) coordinates, "
+                       f"{INGEST_NNZ} nnz, file in the page cache -> device COO tensor"}
+    with tempfile.TemporaryDirectory() as tmp:
+        inds = [i.cpu().numpy() for i in coords_torch(C2_DIMS, INGEST_NNZ, SEED + 21, zipf_s=1.1, device=dev)]
+        rng = np.random.default_rng(SEED + 22)
+        vals = rng.integers(0, 1_000_000, INGEST_NNZ)
+        path = f"{tmp}/c2_10m.tns"
+        write_tns_fixed(path, C2_DIMS, inds, vals)
+        size = os.path.getsize(path)
+        times = []
+        for _ in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            t = DeviceTensor.load(path)
+            times.append(time.perf_counter() - t0)
+            t.free()
+        sec = sorted(times[1:])[len(times[1:]) // 2]
+        out.update({"file_bytes": size, "nnz": INGEST_NNZ, "s_load": round(sec, 4),
+                    "GBps": round(size / sec / 1e9, 3), "Mnnz_per_s": round(INGEST_NNZ / sec / 1e6, 1)})
+        t = DeviceTensor.load(path, dedupe=True)
+        info_inds, _ = t.coo_arrays()
+        out["unique_nnz"] = int(info_inds[0].size)
+        t.free()
+        try:
+            from oracle.oracle import Ref
+            ref = Ref() if Ref.available() else None
+        except Exception:
+            ref = None
+        if ref is not None:
+            rpath = f"{tmp}/c2_1m.tns"
+            write_tns_fixed(rpath, C2_DIMS, [i[:INGEST_REF_NNZ] for i in inds], vals[:INGEST_REF_NNZ])
+            rsize = os.path.getsize(rpath)
+            t0 = time.perf_counter()
+            rc, _, rinds, _ = ref.load(rpath, 1)
+            rsec = time.perf_counter() - t0
+            if rc == 0:
+                out["reference_cpu"] = {"kind": "reference", "cores": 1, "sample": f"first {INGEST_REF_NNZ} nonzeros "
+                                        "of the same file construction, ptiLoadSparseTensor (fscanf)",
+                                        "file_bytes": rsize, "s_load": round(rsec, 3),
+                                        "GBps": round(rsize / rsec / 1e9, 4)}
+                out["speedup_vs_reference"] = round(out["GBps"] / out["reference_cpu"]["GBps"], 1)
+    return out
+
+
 C5_TENSORS = 256
 C5_ITERS = 20
 
@@ -661,7 +743,8 @@ def main():
     ap.add_argument("--no-gradcp", action="store_true", help="skip the gradient-CP (C4) block")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched CPD-ALS (C5) block")
     ap.add_argument("--batched-iters", type=int, default=C5_ITERS)
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched"], default=None,
+    ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest"], default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
                     help="C5 tensors (spread over the size range) checked against the FP64 oracle")
@@ -688,7 +771,7 @@ def main():
     if args.only:
         import torch
         torch.cuda.set_device(0)
-        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched}[args.only]
+        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
         return
     rank, world, _ = dist_setup(args.gpus)
@@ -708,6 +791,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["batched"] = run_batched(args)
+        if world == 1 and not args.no_ingest:
+            import torch
+            torch.cuda.empty_cache()
+            res["ingest"] = run_ingest(args)
         print(json.dumps(res), flush=True)
     from hiparti_b200 import replicas
     replicas.shutdown(world)

@@ -271,6 +271,31 @@ class DeviceTensor:
         return cls(hp[0], t.dims)
 
     @classmethod
+    def load(cls, fname, start_index: int = 1, dedupe: bool = False) -> "DeviceTensor":
+        """ptiB200LoadSparseTensor: a .tns/.bin file parsed on the GPU into a
+        device COO tensor.  dedupe=True sorts by coordinate and sums the values
+        of repeated coordinates (the reference keeps duplicates)."""
+        hp = ffi.new("ptiB200Tensor **")
+        check(lib().ptiB200LoadSparseTensor(hp, start_index, str(fname).encode(), int(bool(dedupe)), ffi.NULL),
+              "ptiB200LoadSparseTensor")
+        info = ffi.new("ptiNnzIndex[7]")
+        dims = ffi.new("ptiIndex[8]")
+        check(lib().ptiB200TensorInfo(hp[0], info, dims), "ptiB200TensorInfo")
+        return cls(hp[0], [dims[m] for m in range(info[0])])
+
+    def coo_arrays(self):
+        """(inds, vals) of a device COO tensor as numpy arrays (ptiB200DownloadCOO)."""
+        info = ffi.new("ptiNnzIndex[7]")
+        dims = ffi.new("ptiIndex[8]")
+        check(lib().ptiB200TensorInfo(self._h, info, dims), "ptiB200TensorInfo")
+        N, nnz = int(info[0]), int(info[1])
+        inds = [np.empty(nnz, np.uint32) for _ in range(N)]
+        vals = np.empty(nnz, np.float32)
+        ip = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", a.ctypes.data) for a in inds])
+        check(lib().ptiB200DownloadCOO(self._h, ip, ffi.cast("ptiValue *", vals.ctypes.data)), "ptiB200DownloadCOO")
+        return inds, vals
+
+    @classmethod
     def from_torch_coo(cls, dims, inds, vals) -> "DeviceTensor":
         """inds: list of int32/uint32-valued CUDA tensors (nnz,), vals: float32 (nnz,)."""
         import torch

@@ -1,9 +1,10 @@
 // containers.cu -- host-side life cycle of the reference's structs and the
-// .tns / .bin tensor reader.  Struct layouts are those of
+// reference's tensor loader (parsed on the GPU, ingest.cu).  Struct layouts are those of
 // include/includes/structs.h in the reference; ownership follows its
 // src/sptensor/sptensor.c, src/matrix/matrix.c, src/ktensor/ktensor.c and
 // src/sptensor/hicoo/hicoo.c.
 #include "common.cuh"
+#include "tensor.cuh"
 
 #include <cerrno>
 #include <cmath>
@@ -28,121 +29,6 @@ void free_vector(V *v)
     std::free(v->data);
     v->data = nullptr;
     v->len = v->cap = 0;
-}
-
-// Reads a whole file into memory.
-int slurp(const char *fname, std::vector<char> &buf)
-{
-    FILE *fp = std::fopen(fname, "rb");
-    PTI_CHECK(fp, PTIERR_OS_ERROR + errno, "SpTns Load", std::strerror(errno));
-    std::fseek(fp, 0, SEEK_END);
-    long n = std::ftell(fp);
-    std::fseek(fp, 0, SEEK_SET);
-    buf.resize(n > 0 ? (size_t)n + 1 : 1);
-    size_t got = n > 0 ? std::fread(buf.data(), 1, (size_t)n, fp) : 0;
-    std::fclose(fp);
-    buf.resize(got + 1);
-    buf[got] = 0;
-    return 0;
-}
-
-// Text coordinate format, src/sptensor/load.c:63-115: "N", then N mode sizes,
-// then one nonzero per line: N indices (start_index-based) and a value.
-int read_text(ptiSparseTensor *tsr, ptiIndex start_index, const std::vector<char> &buf)
-{
-    const char *p = buf.data();
-    char *end = nullptr;
-    unsigned long nm = std::strtoul(p, &end, 10);
-    PTI_CHECK(end != p && nm > 0 && nm < 64, PTIERR_VALUE_ERROR, "SpTns Load", "bad header");
-    p = end;
-    ptiIndex nmodes = (ptiIndex)nm;
-    std::vector<ptiIndex> ndims(nmodes);
-    for (ptiIndex m = 0; m < nmodes; ++m) {
-        unsigned long d = std::strtoul(p, &end, 10);
-        PTI_CHECK(end != p, PTIERR_VALUE_ERROR, "SpTns Load", "bad mode sizes");
-        ndims[m] = (ptiIndex)d;
-        p = end;
-    }
-    std::vector<std::vector<ptiIndex>> inds(nmodes);
-    std::vector<ptiValue> vals;
-    for (;;) {
-        ptiIndex idx[64];
-        bool ok = true;
-        for (ptiIndex m = 0; m < nmodes; ++m) {
-            unsigned long v = std::strtoul(p, &end, 10);
-            if (end == p) { ok = false; break; }
-            p = end;
-            if (v < start_index) PTI_FAIL(PTIERR_VALUE_ERROR, "SpTns Load", "index < start_index");
-            idx[m] = (ptiIndex)(v - start_index);
-        }
-        if (!ok) break;
-        double val = std::strtod(p, &end);
-        if (end == p) break;
-        p = end;
-        for (ptiIndex m = 0; m < nmodes; ++m) inds[m].push_back(idx[m]);
-        vals.push_back((ptiValue)val);
-    }
-    uint64_t nnz = vals.size();
-    tsr->nmodes = nmodes;
-    // The reference's text reader leaves sortorder zero-filled (load.c:69-71).
-    tsr->sortorder = static_cast<ptiIndex *>(std::calloc(nmodes, sizeof(ptiIndex)));
-    tsr->ndims = static_cast<ptiIndex *>(std::malloc(nmodes * sizeof(ptiIndex)));
-    std::memcpy(tsr->ndims, ndims.data(), nmodes * sizeof(ptiIndex));
-    tsr->nnz = nnz;
-    tsr->inds = static_cast<ptiIndexVector *>(std::malloc(nmodes * sizeof(ptiIndexVector)));
-    for (ptiIndex m = 0; m < nmodes; ++m) {
-        PTI_TRY((new_vector<ptiIndexVector, ptiIndex>(&tsr->inds[m], nnz, nnz)));
-        if (nnz) std::memcpy(tsr->inds[m].data, inds[m].data(), nnz * sizeof(ptiIndex));
-    }
-    PTI_TRY((new_vector<ptiValueVector, ptiValue>(&tsr->values, nnz, nnz)));
-    if (nnz) std::memcpy(tsr->values.data, vals.data(), nnz * sizeof(ptiValue));
-    return 0;
-}
-
-// SPLATT binary format, src/sptensor/load.c:120-265: header {int32 magic,
-// uint64 idx_width, uint64 val_width}, then nmodes, dims and nnz as idx_width
-// integers, the indices mode by mode, then the values.
-int read_binary(ptiSparseTensor *tsr, const std::vector<char> &buf)
-{
-    size_t pos = 0, n = buf.size() - 1;
-    auto take = [&](void *dst, size_t bytes) -> bool {
-        if (pos + bytes > n) return false;
-        std::memcpy(dst, buf.data() + pos, bytes);
-        pos += bytes;
-        return true;
-    };
-    int32_t magic;
-    uint64_t iw, vw;
-    PTI_CHECK(take(&magic, 4) && take(&iw, 8) && take(&vw, 8), PTIERR_VALUE_ERROR, "SpTns Load",
-              "truncated header");
-    PTI_CHECK(iw == 4, PTIERR_VALUE_ERROR, "SpTns Load", "only 32-bit indices are supported");
-    PTI_CHECK(vw == 4 || vw == 8, PTIERR_VALUE_ERROR, "SpTns Load", "bad value width");
-    uint32_t nm;
-    PTI_CHECK(take(&nm, 4) && nm > 0 && nm < 64, PTIERR_VALUE_ERROR, "SpTns Load", "bad nmodes");
-    std::vector<ptiIndex> dims(nm);
-    PTI_CHECK(take(dims.data(), 4 * nm), PTIERR_VALUE_ERROR, "SpTns Load", "truncated dims");
-    uint32_t nnz32;
-    PTI_CHECK(take(&nnz32, 4), PTIERR_VALUE_ERROR, "SpTns Load", "truncated nnz");
-    uint64_t nnz = nnz32;
-    PTI_TRY(ptiNewSparseTensor(tsr, nm, dims.data()));
-    tsr->nnz = nnz;
-    for (uint32_t m = 0; m < nm; ++m) {
-        free_vector(&tsr->inds[m]);
-        PTI_TRY((new_vector<ptiIndexVector, ptiIndex>(&tsr->inds[m], nnz, nnz)));
-        PTI_CHECK(take(tsr->inds[m].data, 4 * nnz), PTIERR_VALUE_ERROR, "SpTns Load", "truncated indices");
-    }
-    free_vector(&tsr->values);
-    PTI_TRY((new_vector<ptiValueVector, ptiValue>(&tsr->values, nnz, nnz)));
-    if (vw == 4) {
-        PTI_CHECK(take(tsr->values.data, 4 * nnz), PTIERR_VALUE_ERROR, "SpTns Load", "truncated values");
-    } else {
-        for (uint64_t z = 0; z < nnz; ++z) {
-            double d;
-            PTI_CHECK(take(&d, 8), PTIERR_VALUE_ERROR, "SpTns Load", "truncated values");
-            tsr->values.data[z] = (ptiValue)d;
-        }
-    }
-    return 0;
 }
 
 }  // namespace
@@ -181,13 +67,28 @@ void ptiFreeSparseTensor(ptiSparseTensor *tsr)
 
 int ptiLoadSparseTensor(ptiSparseTensor *tsr, ptiIndex start_index, char const *const fname)
 {
-    PTI_CHECK(fname, PTIERR_VALUE_ERROR, "SpTns Load", "null file name");
-    std::vector<char> buf;
-    PTI_TRY(slurp(fname, buf));
-    // File type by extension, src/sptensor/load.c:28-60.
-    const char *suffix = std::strrchr(fname, '.');
-    bool binary = suffix && std::strcmp(suffix, ".bin") == 0;
-    return binary ? read_binary(tsr, buf) : read_text(tsr, start_index, buf);
+    const char *mod = "SpTns Load";
+    PTI_CHECK(tsr && fname, PTIERR_VALUE_ERROR, mod, "null argument");
+    cudaStream_t s = pti::sync_stream();
+    ptiB200Tensor t;
+    bool text = true;
+    PTI_TRY(pti::ingest_file(&t, start_index, fname, &text, s));
+    PTI_TRY(ptiNewSparseTensor(tsr, t.nmodes, t.ndims.data()));
+    // The reference's text reader leaves sortorder zero-filled (load.c:68-71).
+    if (text) std::memset(tsr->sortorder, 0, t.nmodes * sizeof(ptiIndex));
+    const uint64_t nnz = t.nnz;
+    tsr->nnz = nnz;
+    for (ptiIndex m = 0; m < t.nmodes; ++m) {
+        free_vector(&tsr->inds[m]);
+        PTI_TRY((new_vector<ptiIndexVector, ptiIndex>(&tsr->inds[m], nnz, nnz)));
+        if (nnz)
+            PTI_CUDA(cudaMemcpyAsync(tsr->inds[m].data, t.inds[m].ptr, nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+    }
+    free_vector(&tsr->values);
+    PTI_TRY((new_vector<ptiValueVector, ptiValue>(&tsr->values, nnz, nnz)));
+    if (nnz) PTI_CUDA(cudaMemcpyAsync(tsr->values.data, t.vals.ptr, nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
 }
 
 int ptiNewMatrix(ptiMatrix *mtx, ptiIndex const nrows, ptiIndex const ncols)

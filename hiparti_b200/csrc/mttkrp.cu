@@ -382,9 +382,15 @@ int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s)
     PTI_CUDA(t->vals.alloc(padded(t->nnz * 4), s), mod);
     if (t->nnz)
         PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, X->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s), mod);
+    return check_coo_ranges(t, s);
+}
+
+int check_coo_ranges(ptiB200Tensor *t, cudaStream_t s)
+{
+    const char *mod = "B200 Upload";
     PTI_TRY(ensure_err_word(s));
     if (t->nnz) {
-        for (uint32_t m = 0; m < X->nmodes; ++m)
+        for (uint32_t m = 0; m < t->nmodes; ++m)
             check_coo_kernel<<<grid_for(t->nnz, 256), 256, 0, s>>>(t->inds[m].as<uint32_t>(), t->nnz,
                                                                    t->ndims[m], err_word());
         PTI_CUDA(cudaGetLastError(), mod);

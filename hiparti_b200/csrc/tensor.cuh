@@ -70,6 +70,13 @@ struct ptiB200Tensor {
 namespace pti {
 
 int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
+// Checks every index of a device COO tensor against the mode sizes.
+int check_coo_ranges(ptiB200Tensor *t, cudaStream_t s);
+// Reads a .tns/.coo/.bin file into t's COO arrays on the GPU (ingest.cu);
+// `text` (may be NULL) receives whether the text parser ran.  Synchronous.
+int ingest_file(ptiB200Tensor *t, uint32_t start_index, const char *fname, bool *text, cudaStream_t s);
+// Sorts t's nonzeros by coordinate and merges repeated coordinates.
+int dedupe_coo(ptiB200Tensor *t, cudaStream_t s);
 // With s2, the arrays that mode first_mode's schedule does not need first
 // (the other modes' coordinates and offsets, the values) are copied on s2, and
 // `late` is recorded on s2 after them.

@@ -149,7 +149,9 @@ void ptiFreeSparseTensor(ptiSparseTensor *tsr);
 /* include/includes/sptensors.h:26 (sum of squared values, FP64 accumulation; GPU) */
 double SparseTensorFrobeniusNormSquared(ptiSparseTensor const * const ptien);
 /* include/includes/sptensors.h:27 -- text .tns (header "N\nI_0 ... I_{N-1}")
- * or SPLATT .bin, selected by file extension as in src/sptensor/load.c:277-297 */
+ * or SPLATT .bin, selected by file extension as in src/sptensor/load.c:277-297.
+ * The file is parsed on the GPU (see ptiB200LoadSparseTensor); the nonzeros,
+ * their order and their values are those of the reference's fscanf reader. */
 int  ptiLoadSparseTensor(ptiSparseTensor *tsr, ptiIndex start_index, char const * const fname);
 
 /* include/includes/matrices.h:26-34 */
@@ -280,6 +282,22 @@ int ptiB200DownloadHiCOO(ptiB200Tensor const *t, ptiNnzIndex *bptr, void * const
                          void * const *einds, ptiValue *vals);
 /* Shape and statistics of a device tensor.  info: [nmodes, nnz, nb, sb, sk, sc, is_hicoo]. */
 int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndims_out);
+
+/* Loads a tensor file straight into device memory: the bytes are copied to
+ * the GPU and parsed there (the reference parses on the host,
+ * src/sptensor/load.c:63-265).  File types and results are those of
+ * ptiLoadSparseTensor: .bin is SPLATT binary, other names are text
+ * coordinates with 1-based (start_index 1) or 0-based indices; duplicates are
+ * kept unless dedupe != 0, which sorts the nonzeros by coordinate (mode 0
+ * first) and replaces each repeated coordinate by one nonzero holding the FP32
+ * sum of its values in file order.  Indices must fit the mode sizes.  Hex
+ * values, nan(...) payloads, values with more than 100 significant digits and
+ * tokens longer than 4096 bytes are rejected.  Synchronous on `stream`. */
+int ptiB200LoadSparseTensor(ptiB200Tensor **out, ptiIndex start_index, const char *fname, int dedupe,
+                            void *stream);
+/* Copies a device COO tensor's arrays to host buffers: inds[m] and vals, nnz
+ * entries each (NULL entries are skipped).  Synchronous. */
+int ptiB200DownloadCOO(ptiB200Tensor const *t, ptiIndex * const *inds, ptiValue *vals);
 
 /* MTTKRP with everything in device memory.  dev_mats[k] points to ndims[k] x
  * stride row-major factors of element type `factor_type`; dev_out receives

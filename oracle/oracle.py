@@ -240,6 +240,19 @@ class Ref:
         self.L.CpdAlsStep.restype = C.c_double
         self.L.OmpCpdAlsStep.restype = C.c_double
 
+    def load(self, fname, start_index=1):
+        """ptiLoadSparseTensor of the reference.  Returns (rc, dims, inds, vals)."""
+        t = _SpTensor()
+        rc = self.L.ptiLoadSparseTensor(C.byref(t), C.c_uint32(start_index), str(fname).encode())
+        if rc != 0:
+            return rc, None, None, None
+        N, nnz = int(t.nmodes), int(t.nnz)
+        dims = list(_np_from(t.ndims, N, np.uint32))
+        inds = [_np_from(t.inds[m].data, nnz, np.uint32) for m in range(N)]
+        vals = _np_from(t.values.data, nnz, np.float32)
+        self.L.ptiFreeSparseTensor(C.byref(t))
+        return 0, dims, inds, vals
+
     # A COO tensor whose arrays point into numpy buffers owned by `keep`.
     def _coo(self, dims, inds, vals):
         N = len(inds)

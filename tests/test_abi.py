@@ -1,6 +1,6 @@
 """CPU: the C-ABI library loads, exports every entry point the header declares,
 lays out the reference's structs byte for byte, and runs its host-side logic
-(containers, the .tns/.bin reader, argument checks) without a GPU."""
+(containers, argument checks) without a GPU."""
 import re
 import struct
 
@@ -60,36 +60,6 @@ def test_matrix_life_cycle(lib):
     assert lib.ptiConstantMatrix(m, 2.5) == 0
     assert m.values[4 * 16 + 10] == 2.5
     lib.ptiFreeMatrix(m)
-
-
-def test_load_tns_and_bin(lib, tmp_path):
-    p = tmp_path / "t.tns"
-    p.write_text("3\n4 5 6\n1 1 1 1.5\n4 5 6 -2.0\n2 3 1 0.25\n")
-    t = COOTensor.load(str(p))
-    assert t.dims == [4, 5, 6] and t.nnz == 3
-    np.testing.assert_array_equal(t.inds[0], [0, 3, 1])
-    np.testing.assert_array_equal(t.inds[2], [0, 5, 0])
-    np.testing.assert_array_equal(t.vals, np.float32([1.5, -2.0, 0.25]))
-    # SPLATT binary: header, nmodes, dims, nnz, indices per mode, values
-    b = tmp_path / "t.bin"
-    with open(b, "wb") as f:
-        f.write(struct.pack("<iQQ", 0, 4, 4))
-        f.write(struct.pack("<I", 3) + struct.pack("<3I", 4, 5, 6) + struct.pack("<I", 2))
-        f.write(struct.pack("<2I", 0, 3) + struct.pack("<2I", 1, 4) + struct.pack("<2I", 5, 0))
-        f.write(struct.pack("<2f", 1.0, 2.0))
-    tb = COOTensor.load(str(b))
-    assert tb.dims == [4, 5, 6]
-    np.testing.assert_array_equal(tb.inds[1], [1, 4])
-    np.testing.assert_array_equal(tb.vals, np.float32([1, 2]))
-
-
-def test_load_reference_fixture_if_present(lib):
-    from pathlib import Path
-    f = Path("/root/reference/data/tensors/3d_7.tns")
-    if not f.exists():
-        pytest.skip("reference data not mounted")
-    t = COOTensor.load(str(f))
-    assert t.nmodes == 3 and t.nnz == 9
 
 
 def test_shape_mismatch_is_reported_before_any_gpu_work(lib):

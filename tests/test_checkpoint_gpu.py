@@ -1,10 +1,13 @@
 """GPU tests of CPD-ALS checkpoint / resume (ptiB200CpdAlsCheckpoint).
 
 A run stopped after k iterations and resumed from its checkpoint must follow
-the uninterrupted run: the restored fits are the stored ones bit for bit, the
-later fits agree within 1e-5 (the two runs add MTTKRP contributions with FP32
-atomics in different orders), weights and factors within relative 1e-3, and
-both stay within 1e-4 of the FP64 oracle's fit."""
+the uninterrupted run.  The restored fits are the stored ones bit for bit.  Two
+runs differ only in the order of their FP32 atomic additions, so later fits
+agree within 1e-5 and weights and factors within relative 1e-3 (FP32
+factors).  With BF16 factor copies, such a last-bit difference can flip the
+rounding of a BF16 element (2^-8 relative), so there the bounds are 1e-4 and
+1e-2.  The FP32 runs also stay within 1e-4 of the FP64 oracle's fit.  The test
+tensor has exact CP rank R, so ALS converges and the factors are determined."""
 import numpy as np
 import pytest
 
@@ -19,7 +22,7 @@ R = 8
 
 @pytest.fixture(scope="module")
 def problem():
-    inds, vals, _ = synth.planted_tensor(DIMS, 40000, 5, 0.01, seed=11)
+    inds, vals, _ = synth.sparse_lowrank_tensor(DIMS, R, 20, noise=0.05, seed=11)
     rng = np.random.default_rng(12)
     init = [np.abs(rng.standard_normal((d, R))).astype(np.float32) for d in DIMS]
     return inds, vals, init
@@ -53,7 +56,7 @@ def _run(dt, init, iters, scale=1.0, **kw):
 @pytest.mark.parametrize("precision", ["fp32", "bf16"])
 def test_resume_follows_uninterrupted_run(lib, cuda, orc, tmp_path, problem, fmt, precision):
     inds, vals, init = problem
-    total, stop = 30, 12
+    total, stop = 30, 7
     dt = _device(inds, vals, fmt)
     # No closing FP32 sweeps: the stopped run must take the same BF16/FP32
     # schedule as the first `stop` iterations of the whole run.
@@ -77,10 +80,12 @@ def test_resume_follows_uninterrupted_run(lib, cuda, orc, tmp_path, problem, fmt
     dt.free()
     assert len(fits_c) == total
     assert fits_c[:stop] == fits_b
-    np.testing.assert_allclose(fits_c, fits_a, atol=1e-5, rtol=0)
-    assert rel_err(lam_c, lam_a) < 1e-3
+    fit_tol, fac_tol = (1e-5, 1e-3) if precision == "fp32" else (1e-4, 1e-2)
+    np.testing.assert_allclose(fits_c, fits_a, atol=fit_tol, rtol=0)
+    assert fits_a[-1] > 0.98  # BF16-only iterations reach about 0.99
+    assert rel_err(lam_c, lam_a) < fac_tol
     for a, c in zip(fac_a, fac_c):
-        assert rel_err(c, a) < 1e-3
+        assert rel_err(c, a) < fac_tol
     if precision == "fp32":
         o = orc.cpd_als(list(DIMS), inds, vals, R, total, init)
         assert abs(fits_c[-1] - o["fit"]) < 1e-4
