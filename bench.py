@@ -317,6 +317,85 @@ def run_gradcp(args):
             "ms_per_gradient": round(ms, 3), "loss": float(loss.item())}
 
 
+RENUM_REF_NNZ = 200_000
+
+
+def run_renumber(args):
+    """Lexi-order renumbering (one iteration) of the C2 tensor on the GPU: the
+    HiCOO block count and the all-mode MTTKRP time before and after, the
+    renumbering time, and the reference's orderit (oracle/_ref, CPU) against
+    the GPU on a 200k-nonzero sample of the same construction."""
+    import numpy as np
+    import torch
+    from hiparti_b200 import COOTensor
+    dev = torch.device("cuda", torch.cuda.current_device())
+    coo, h, inds, vals, _ = make_c2(dev, SEED + 31)
+    facs = c2_factors(dev, SEED + 31)
+
+    def mttkrp_ms(t):
+        for m in range(3):
+            t.prepare(m)
+        for m in range(3):
+            t.mttkrp(facs, m, rank=C2_R)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            for m in range(3):
+                t.mttkrp(facs, m, rank=C2_R)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 3
+
+    out = {"workload": "Lexi-order renumbering, 1 iteration, of the C2 tensor (3-D 200000x150000x20000, 50M "
+                       "Zipf(1.1) nnz); HiCOO sb=7; MTTKRP R=32 FP32, all 3 modes"}
+    nb0, ms0 = h.nb, mttkrp_ms(h)
+    h.free()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    coo.renumber(1, apply=True)
+    torch.cuda.synchronize()
+    ren_s = time.perf_counter() - t0
+    h2 = coo.to_hicoo(C2_SB, C2_SK, C2_SC)
+    nb1, ms1 = h2.nb, mttkrp_ms(h2)
+    h2.free()
+    coo.free()
+    out.update({"s_renumber_gpu": round(ren_s, 3), "nb_before": nb0, "nb_after": nb1,
+                "nnz_per_block_before": round(C2_NNZ / nb0, 2), "nnz_per_block_after": round(C2_NNZ / nb1, 2),
+                "mttkrp_ms_all_modes_before": round(ms0, 3), "mttkrp_ms_all_modes_after": round(ms1, 3)})
+    try:
+        from oracle.oracle import Ref
+        ref = Ref() if Ref.available() else None
+    except Exception:
+        ref = None
+    if ref is not None:
+        sample = [i[:RENUM_REF_NNZ].cpu().numpy() for i in inds]
+        keys = np.unique(np.stack(sample, 1), axis=0)  # orderit wants unique coordinates
+        sinds = [keys[:, m].astype(np.uint32) for m in range(3)]
+        svals = np.ones(keys.shape[0], np.float32)
+        import os as _os
+        t0 = time.perf_counter()
+        devnull = _os.open(_os.devnull, _os.O_WRONLY)
+        saved = _os.dup(1)
+        _os.dup2(devnull, 1)  # the reference prints per-mode timings
+        try:
+            want = ref.orderit(C2_DIMS, sinds, svals, 1)
+        finally:
+            _os.dup2(saved, 1)
+            _os.close(devnull)
+            _os.close(saved)
+        ref_s = time.perf_counter() - t0
+        small = COOTensor(C2_DIMS, sinds, svals)
+        small.renumber(1)  # warm-up
+        t0 = time.perf_counter()
+        got = small.renumber(1)
+        ours_s = time.perf_counter() - t0
+        out["sample"] = {"nnz": int(keys.shape[0]), "s_reference_orderit_cpu": round(ref_s, 3),
+                         "s_ours_gpu_incl_copies": round(ours_s, 4),
+                         "identical_to_reference": bool(all(np.array_equal(a, b) for a, b in zip(got, want)))}
+    return out
+
+
 INGEST_NNZ = 10_000_000
 INGEST_REF_NNZ = 1_000_000
 
@@ -744,7 +823,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched CPD-ALS (C5) block")
     ap.add_argument("--batched-iters", type=int, default=C5_ITERS)
     ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest"], default=None,
+    ap.add_argument("--no-renumber", action="store_true", help="skip the renumbering block")
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber"], default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
                     help="C5 tensors (spread over the size range) checked against the FP64 oracle")
@@ -771,7 +851,8 @@ def main():
     if args.only:
         import torch
         torch.cuda.set_device(0)
-        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest}[args.only]
+        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
+                 "renumber": run_renumber}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
         return
     rank, world, _ = dist_setup(args.gpus)
@@ -795,6 +876,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["ingest"] = run_ingest(args)
+        if world == 1 and not args.no_renumber:
+            import torch
+            torch.cuda.empty_cache()
+            res["renumber"] = run_renumber(args)
         print(json.dumps(res), flush=True)
     from hiparti_b200 import replicas
     replicas.shutdown(world)

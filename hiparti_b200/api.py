@@ -110,6 +110,26 @@ class COOTensor:
     def cpd_als(self, R, niters, tol=0.0, variant="seq"):
         return _host_cpd(self, R, niters, tol, variant)
 
+    def renumber(self, iterations=1):
+        """Lexi-order renumbering (ptiIndexRenumber, computed on the GPU):
+        per mode, original index -> new index.  The tensor is not changed."""
+        maps = [np.empty(d, np.uint32) for d in self.dims]
+        mp = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", m.ctypes.data) for m in maps])
+        lib().ptiClearLastError()
+        lib().ptiIndexRenumber(self.c, mp, 1, int(iterations), 7, 1, 1)
+        code = lib().ptiGetLastError(ffi.NULL, ffi.NULL, ffi.NULL, ffi.NULL)
+        if code:
+            raise PtiError(code, "ptiIndexRenumber")
+        return maps
+
+    def shuffled(self, maps):
+        """A copy with every coordinate replaced by maps[m][old] (ptiSparseTensorShuffleIndices)."""
+        t = COOTensor(self.dims, [i.copy() for i in self.inds], self.vals.copy())
+        keep = [np.ascontiguousarray(m, np.uint32) for m in maps]
+        mp = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", m.ctypes.data) for m in keep])
+        lib().ptiSparseTensorShuffleIndices(t.c, mp)
+        return t
+
 
 class HiCOOTensor:
     """A HiCOO tensor held as numpy arrays (the fields of ptiSparseTensorHiCOO)."""
@@ -410,6 +430,15 @@ class DeviceTensor:
                                             int(checkpoint_every), int(bool(resume)), stream),
               "ptiB200CpdAlsCheckpoint")
         return lam, [fits[i] for i in range(done[0])]
+
+    def renumber(self, iterations=1, apply=True):
+        """Lexi-order renumbering on the GPU (ptiB200Renumber): per mode,
+        original index -> new index; apply=True renumbers this tensor's
+        coordinates in place."""
+        maps = [np.empty(d, np.uint32) for d in self.dims]
+        mp = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", m.ctypes.data) for m in maps])
+        check(lib().ptiB200Renumber(self._h, int(iterations), mp, int(bool(apply)), ffi.NULL), "ptiB200Renumber")
+        return maps
 
     def free(self):
         if self._h is not None:

@@ -154,11 +154,30 @@ double SparseTensorFrobeniusNormSquared(ptiSparseTensor const * const ptien);
  * their order and their values are those of the reference's fscanf reader. */
 int  ptiLoadSparseTensor(ptiSparseTensor *tsr, ptiIndex start_index, char const * const fname);
 
+/* include/includes/sptensors.h:100 -- Lexi-order renumbering (renumber == 1)
+ * on the GPU; newIndices[m][old] = new.  tsr is not modified.  sb_bits and tk
+ * are unused; impl_num 0 or 1.  Other choices record PTIERR_VALUE_ERROR (see
+ * ptiGetLastError) and leave the identity in newIndices. */
+void ptiIndexRenumber(ptiSparseTensor * tsr, ptiIndex ** newIndices, int renumber, ptiIndex iterations,
+                      ptiElementIndex sb_bits, int tk, int impl_num);
+/* include/includes/sptensors.h:101, src/sptensor/orderit.c:121-208 -- the same
+ * Lexi-order.  (The reference's ptiIndexRenumber sorts the nonzeros with a
+ * defective insertion sort and so depends on their order; both entry points
+ * here give orderit's result.) */
+void orderit(ptiSparseTensor *tsr, ptiIndex **newIndices, int const renumber, ptiIndex const iterations);
+/* include/includes/sptensors.h:45 -- coordinates replaced by map_inds[m][old] */
+void ptiSparseTensorShuffleIndices(ptiSparseTensor *tsr, ptiIndex ** map_inds);
+
 /* include/includes/matrices.h:26-34 */
 int  ptiNewMatrix(ptiMatrix *mtx, ptiIndex const nrows, ptiIndex const ncols);
 int  ptiRandomizeMatrix(ptiMatrix *mtx);           /* A[i,j] = i+j+1, src/matrix/matrix.c:67-74 */
 int  ptiConstantMatrix(ptiMatrix * const mtx, ptiValue const val);
 void ptiFreeMatrix(ptiMatrix *mtx);
+
+/* include/includes/matrices.h:30, ktensors.h:24 -- row i becomes row map[i]
+ * (factors of a renumbered tensor back in the original numbering) */
+void ptiMatrixInverseShuffleIndices(ptiMatrix *mtx, ptiIndex * mode_map_inds);
+void ptiKruskalTensorInverseShuffleIndices(ptiKruskalTensor * ktsr, ptiIndex ** map_inds);
 
 /* include/includes/ktensors.h:23-25 */
 int  ptiNewKruskalTensor(ptiKruskalTensor *ktsr, ptiIndex nmodes, const ptiIndex ndims[], ptiIndex rank);
@@ -298,6 +317,17 @@ int ptiB200LoadSparseTensor(ptiB200Tensor **out, ptiIndex start_index, const cha
 /* Copies a device COO tensor's arrays to host buffers: inds[m] and vals, nnz
  * entries each (NULL entries are skipped).  Synchronous. */
 int ptiB200DownloadCOO(ptiB200Tensor const *t, ptiIndex * const *inds, ptiValue *vals);
+
+/* Lexi-order renumbering of a device COO tensor on the GPU (the reference runs
+ * it on the host, src/sptensor/renumber.c:26-92).  Each mode in turn, for
+ * `iterations` rounds, gets its indices ordered by the lexicographic order of
+ * their row lists in the matricisation against the other modes (an index
+ * present in the first differing row comes first; indices without nonzeros
+ * come last; equal lists keep their current order).  new_indices (host, may be
+ * NULL or hold NULL entries) receives original index -> new index per mode.
+ * apply != 0 also renumbers the tensor's coordinates in place.  Synchronous. */
+int ptiB200Renumber(ptiB200Tensor *t, ptiIndex iterations, ptiIndex * const *new_indices, int apply,
+                    void *stream);
 
 /* MTTKRP with everything in device memory.  dev_mats[k] points to ndims[k] x
  * stride row-major factors of element type `factor_type`; dev_out receives

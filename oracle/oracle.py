@@ -184,6 +184,43 @@ class Orc:
 # ----------------------------------------------------------------------------
 # The reference library (compiled from its own sources)
 # ----------------------------------------------------------------------------
+def lexi_order(dims, inds, iterations):
+    """Lexi-order renumbering restated (src/sptensor/renumber.c:26-92,
+    403-520; lexOrderThem :93-225).  For each mode in turn, `iterations` times:
+    rows are the other modes' coordinate tuples in lexicographic order (the
+    other modes ascending), each index's list is its rows in ascending order,
+    and the indices are ordered by their lists, where at the first differing
+    row the index present in that row comes first (a list precedes its own
+    prefixes; indices without nonzeros come last).  This is the order the
+    reference's partition refinement over the rows yields.  Indices with equal
+    lists keep their current order.  Pure Python: small tensors only.
+    Returns newIndices (per mode, original index -> new index)."""
+    N = len(dims)
+    cur = [np.asarray(i, np.int64).copy() for i in inds]
+    org = [np.arange(d) for d in dims]          # current index -> original
+    nnz = cur[0].size
+    for _ in range(iterations):
+        for m in range(N):
+            others = [k for k in range(N) if k != m]
+            tuples = sorted({tuple(int(cur[k][z]) for k in others) for z in range(nnz)})
+            rid = {t: r for r, t in enumerate(tuples)}
+            lists = [[] for _ in range(dims[m])]
+            for z in range(nnz):
+                lists[int(cur[m][z])].append(rid[tuple(int(cur[k][z]) for k in others)])
+            inf = len(tuples)
+            order = sorted(range(dims[m]), key=lambda c: (tuple(sorted(lists[c])) + (inf,), c))
+            inv = np.empty(dims[m], np.int64)
+            inv[np.asarray(order, np.int64)] = np.arange(dims[m])
+            cur[m] = inv[cur[m]]
+            org[m] = org[m][np.asarray(order, np.int64)]
+    out = []
+    for m in range(N):
+        mp = np.empty(dims[m], np.uint32)
+        mp[org[m]] = np.arange(dims[m], dtype=np.uint32)
+        out.append(mp)
+    return out
+
+
 class _Vec(C.Structure):
     _fields_ = [("len", C.c_uint64), ("cap", C.c_uint64), ("data", C.c_void_p)]
 
@@ -252,6 +289,24 @@ class Ref:
         vals = _np_from(t.values.data, nnz, np.float32)
         self.L.ptiFreeSparseTensor(C.byref(t))
         return 0, dims, inds, vals
+
+    def renumber(self, dims, inds, vals, iterations, impl_num=1):
+        """ptiIndexRenumber(renumber=1) of the reference: newIndices per mode."""
+        t, keep = self._coo(dims, inds, vals)
+        maps = [np.zeros(d, np.uint32) for d in dims]
+        arr = (C.c_void_p * len(dims))(*[m.ctypes.data for m in maps])
+        self.L.ptiIndexRenumber(C.byref(t), arr, C.c_int(1), C.c_uint32(iterations), C.c_uint8(7), C.c_int(1),
+                                C.c_int(impl_num))
+        return maps
+
+    def orderit(self, dims, inds, vals, iterations):
+        """orderit(renumber=1) of the reference (src/sptensor/orderit.c:121-208),
+        its Lexi-order driver with a correct coordinate sort."""
+        t, keep = self._coo(dims, inds, vals)
+        maps = [np.zeros(d, np.uint32) for d in dims]
+        arr = (C.c_void_p * len(dims))(*[m.ctypes.data for m in maps])
+        self.L.orderit(C.byref(t), arr, C.c_int(1), C.c_uint32(iterations))
+        return maps
 
     # A COO tensor whose arrays point into numpy buffers owned by `keep`.
     def _coo(self, dims, inds, vals):
