@@ -110,6 +110,41 @@ class COOTensor:
     def cpd_als(self, R, niters, tol=0.0, variant="seq"):
         return _host_cpd(self, R, niters, tol, variant)
 
+    def _semi_sparse(self, Y):
+        N, nf, st = Y.nmodes, Y.nnz, Y.stride
+        inds = [np.frombuffer(ffi.buffer(Y.inds[m].data, 4 * Y.inds[m].len), np.uint32).copy()
+                if Y.inds[m].len else np.empty(0, np.uint32) for m in range(N)]
+        vals = (np.frombuffer(ffi.buffer(Y.values.values, 4 * nf * st), np.float32).reshape(nf, st).copy()
+                if nf else np.empty((0, st), np.float32))
+        lib().ptiFreeSemiSparseTensor(Y)
+        return {"mode": int(Y.mode), "inds": inds, "vals": vals}
+
+    def ttm(self, U, mode):
+        """ptiSparseTensorMulMatrix: returns {"mode", "inds" (fiber coordinates
+        per mode, the mode's own empty), "vals" (nfibers x stride)}.  As in the
+        reference, this tensor's arrays are left sorted with `mode` last."""
+        U = np.ascontiguousarray(U, np.float32)
+        I, R = U.shape
+        st = ((R - 1) // 8 + 1) * 8
+        buf = np.zeros((I, st), np.float32)
+        buf[:, :R] = U
+        m = ffi.new("ptiMatrix *")
+        m.nrows, m.ncols, m.cap, m.stride = I, R, I, st
+        m.values = _ptr(buf, "ptiValue *")
+        Y = ffi.new("ptiSemiSparseTensor *")
+        check(lib().ptiSparseTensorMulMatrix(Y, self.c, m, mode), "ptiSparseTensorMulMatrix")
+        return self._semi_sparse(Y)
+
+    def ttv(self, v, mode):
+        """ptiSparseTensorMulVector (same result layout as ttm, width 1)."""
+        v = np.ascontiguousarray(v, np.float32)
+        vec = ffi.new("ptiValueVector *")
+        vec.len = vec.cap = v.size
+        vec.data = _ptr(v, "ptiValue *")
+        Y = ffi.new("ptiSemiSparseTensor *")
+        check(lib().ptiSparseTensorMulVector(Y, self.c, vec, mode), "ptiSparseTensorMulVector")
+        return self._semi_sparse(Y)
+
     def renumber(self, iterations=1):
         """Lexi-order renumbering (ptiIndexRenumber, computed on the GPU):
         per mode, original index -> new index.  The tensor is not changed."""
@@ -430,6 +465,30 @@ class DeviceTensor:
                                             int(checkpoint_every), int(bool(resume)), stream),
               "ptiB200CpdAlsCheckpoint")
         return lam, [fits[i] for i in range(done[0])]
+
+    def ttm(self, U, mode, rank=None):
+        """TTM along `mode` on the device (ptiB200TTM).  U: CUDA float32
+        (ndims[mode], ldu); rank columns used (default all; 0 = TTV with U's
+        first column read as a vector, ldu 1).  Returns
+        (fiber coordinates per mode as CUDA int32 tensors, the mode's own
+        None; Y as a (nfibers, ldy) CUDA float32 tensor, ldy = rank rounded up
+        to 8)."""
+        import torch
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        R = U.shape[1] if rank is None else int(rank)
+        ldy = ((max(R, 1) - 1) // 8 + 1) * 8  # rank 0 (TTV): one column
+        nf = ffi.new("ptiNnzIndex *")
+        N = len(self.dims)
+        check(lib().ptiB200TTMFibers(self._h, mode, nf, ffi.NULL, stream), "ptiB200TTMFibers")
+        finds = [None if m == mode else torch.empty(int(nf[0]), dtype=torch.int32, device=U.device)
+                 for m in range(N)]
+        fp = ffi.new("ptiIndex *[]", [ffi.NULL if f is None else ffi.cast("ptiIndex *", f.data_ptr())
+                                      for f in finds])
+        check(lib().ptiB200TTMFibers(self._h, mode, nf, fp, stream), "ptiB200TTMFibers")
+        Y = torch.empty((int(nf[0]), ldy), dtype=torch.float32, device=U.device)
+        check(lib().ptiB200TTM(self._h, mode, ffi.cast("float *", U.data_ptr()), R, U.shape[1],
+                               ffi.cast("float *", Y.data_ptr()), ldy, stream), "ptiB200TTM")
+        return finds, Y
 
     def renumber(self, iterations=1, apply=True):
         """Lexi-order renumbering on the GPU (ptiB200Renumber): per mode,

@@ -274,7 +274,10 @@ int renumber_device(ptiB200Tensor *t, uint32_t iterations, uint32_t *const *maps
     for (uint32_t m = 0; m < N; ++m)
         if (maps && maps[m]) final_map_k<<<grid_n(t->ndims[m]), 256, 0, s>>>(org[m].as<uint32_t>(), t->ndims[m], maps[m]);
     PTI_CUDA(cudaGetLastError(), mod);
-    if (apply) t->coo_plan = {};  // schedules built for the old numbering
+    if (apply) {  // schedules built for the old numbering
+        t->coo_plan = {};
+        t->fiber_plan = {};
+    }
     return 0;
 }
 

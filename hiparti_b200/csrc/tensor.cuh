@@ -41,6 +41,18 @@ struct CooModePlan {
     DevBuf alt_vals;                      // float [nnz]: caller-supplied values in record order
 };
 
+// Fibers of a COO tensor along one mode (TTM / TTV): the nonzeros sorted by
+// the other modes with the mode last, cut where any other mode changes.
+struct FiberPlan {
+    bool ready = false;
+    uint64_t nfib = 0;
+    DevBuf fptr;                           // uint64 [nfib+1]: first nonzero of each fiber
+    std::array<DevBuf, kMaxModes> finds;   // uint32 [nfib]: the fiber's coordinate in every other mode
+    DevBuf sind;                           // uint32 [nnz]: the mode's index, fiber order
+    DevBuf sval;                           // float  [nnz]: values, fiber order
+    DevBuf perm;                           // uint32 [nnz]: fiber-order position -> input nonzero
+};
+
 }  // namespace pti
 
 struct ptiB200Tensor {
@@ -65,6 +77,7 @@ struct ptiB200Tensor {
 
     std::array<pti::CooModePlan, pti::kMaxModes> coo_plan;
     std::array<pti::HicooModePlan, pti::kMaxModes> hicoo_plan;
+    std::array<pti::FiberPlan, pti::kMaxModes> fiber_plan;
 };
 
 namespace pti {

@@ -130,6 +130,18 @@ typedef struct {
     ptiRankMatrix **factors;
 } ptiRankKruskalTensor;
 
+/* Semi-sparse tensor (structs.h:219-233): dense along `mode`, sparse in the
+ * other modes -- a sparse tensor of dense fibers.  inds[mode] is empty. */
+typedef struct {
+    ptiIndex nmodes;
+    ptiIndex *ndims;
+    ptiIndex mode;
+    ptiNnzIndex nnz;           /* fibers */
+    ptiIndexVector *inds;      /* [nmodes][nnz] fiber coordinates      */
+    ptiIndex stride;           /* ndims[mode] rounded up to 8          */
+    ptiMatrix values;          /* nnz x stride                         */
+} ptiSemiSparseTensor;
+
 /* ---------------------------------------------------------------------------
  * Error reporting: include/includes/helper_funcs.h:29-30,39-40.
  * A failing call records (module, file, line, reason) in a thread-local slot
@@ -213,6 +225,28 @@ void ptiFreeSparseTensorHiCOO(ptiSparseTensorHiCOO *hitsr);
 int  ptiSparseTensorToHiCOO(ptiSparseTensorHiCOO *hitsr, ptiNnzIndex *max_nnzb, ptiSparseTensor *tsr,
                             const ptiElementIndex sb_bits, const ptiElementIndex sk_bits,
                             const ptiElementIndex sc_bits, int const tk);
+
+/* ---------------------------------------------------------------------------
+ * TTM / TTV along one mode (include/includes/sptensors.h:156-161,
+ * src/sptensor/mmul.c:36-86, vmul.c:26-70).  Y must be uninitialised; it is
+ * created here (release it with ptiFreeSemiSparseTensor).  As in the
+ * reference, X is sorted in place with `mode` last unless its sortorder
+ * already says so, and each fiber's sum runs in that order with FP32
+ * multiply-then-add, so Y is bit-identical to the reference's for distinct
+ * coordinates.  All variants run the same GPU code (impl_num, smen_size
+ * ignored); U has at most 256 columns.
+ * ------------------------------------------------------------------------ */
+int ptiNewSemiSparseTensor(ptiSemiSparseTensor *tsr, ptiIndex nmodes, ptiIndex mode, const ptiIndex ndims[]);
+void ptiFreeSemiSparseTensor(ptiSemiSparseTensor *tsr);
+int ptiSparseTensorMulMatrix(ptiSemiSparseTensor *Y, ptiSparseTensor * const X, ptiMatrix *const U, ptiIndex mode);
+int ptiOmpSparseTensorMulMatrix(ptiSemiSparseTensor *Y, ptiSparseTensor * const X, ptiMatrix * const U,
+                                ptiIndex mode);
+int ptiCudaSparseTensorMulMatrix(ptiSemiSparseTensor *Y, ptiSparseTensor *X, const ptiMatrix *U, ptiIndex const mode);
+int ptiCudaSparseTensorMulMatrixOneKernel(ptiSemiSparseTensor *Y, ptiSparseTensor *X, const ptiMatrix *U,
+                                          ptiIndex const mode, ptiIndex const impl_num,
+                                          ptiNnzIndex const smen_size);
+int ptiSparseTensorMulVector(ptiSemiSparseTensor *Y, ptiSparseTensor * const X, ptiValueVector * const V,
+                             ptiIndex mode);
 
 /* ---------------------------------------------------------------------------
  * MTTKRP.  mats[0..N-1] are the factor matrices (row i of mats[k] is the rank-R
@@ -317,6 +351,18 @@ int ptiB200LoadSparseTensor(ptiB200Tensor **out, ptiIndex start_index, const cha
 /* Copies a device COO tensor's arrays to host buffers: inds[m] and vals, nnz
  * entries each (NULL entries are skipped).  Synchronous. */
 int ptiB200DownloadCOO(ptiB200Tensor const *t, ptiIndex * const *inds, ptiValue *vals);
+
+/* TTM on a device COO tensor.  The fibers along `mode` (nonzeros sorted
+ * with `mode` last, cut where another mode changes) are built on first use
+ * and kept.  ptiB200TTMFibers returns their count and copies their
+ * coordinates (dev_fiber_inds[m], nfibers uint32 each; NULL entries and the
+ * mode itself skipped).  ptiB200TTM writes dev_Y (nfibers x ldy FP32, pad
+ * columns zero) = fibers times dev_U (rows of ldu floats, rank <= 256 columns
+ * used); rank == 0 is TTV with dev_U a vector.  Asynchronous on `stream`. */
+int ptiB200TTMFibers(ptiB200Tensor *t, ptiIndex mode, ptiNnzIndex *nfibers, ptiIndex * const *dev_fiber_inds,
+                     void *stream);
+int ptiB200TTM(ptiB200Tensor *t, ptiIndex mode, const float *dev_U, ptiIndex rank, ptiIndex ldu, float *dev_Y,
+               ptiIndex ldy, void *stream);
 
 /* Lexi-order renumbering of a device COO tensor on the GPU (the reference runs
  * it on the host, src/sptensor/renumber.c:26-92).  Each mode in turn, for

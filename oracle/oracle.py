@@ -254,6 +254,11 @@ class _HiCOO(C.Structure):
 assert C.sizeof(_HiCOO) == 224 and C.sizeof(_SpTensor) == 64 and C.sizeof(_Matrix) == 24
 
 
+class _SemiSparse(C.Structure):
+    _fields_ = [("nmodes", C.c_uint32), ("ndims", C.c_void_p), ("mode", C.c_uint32), ("nnz", C.c_uint64),
+                ("inds", C.POINTER(_Vec)), ("stride", C.c_uint32), ("values", _Matrix)]
+
+
 def _np_from(ptr, n, dtype):
     if n == 0:
         return np.empty(0, dtype)
@@ -298,6 +303,34 @@ class Ref:
         self.L.ptiIndexRenumber(C.byref(t), arr, C.c_int(1), C.c_uint32(iterations), C.c_uint8(7), C.c_int(1),
                                 C.c_int(impl_num))
         return maps
+
+    def ttm(self, dims, inds, vals, U, mode, sortorder=None, vector=False):
+        """ptiSparseTensorMulMatrix (or, with vector=True and U a vector,
+        ptiSparseTensorMulVector) of the reference.  Returns (fiber inds per
+        mode, Y values nfibers x stride, X's arrays after the call, X's
+        sortorder after the call)."""
+        t, keep = self._coo(dims, inds, vals)
+        if sortorder is not None:
+            keep["sortorder"][:] = sortorder
+        Y = _SemiSparse()
+        if vector:
+            v = np.ascontiguousarray(U, np.float32)
+            vec = _Vec(v.size, v.size, v.ctypes.data)
+            rc = self.L.ptiSparseTensorMulVector(C.byref(Y), C.byref(t), C.byref(vec), C.c_uint32(mode))
+        else:
+            R = U.shape[1]
+            st = ((R - 1) // 8 + 1) * 8
+            buf = np.zeros((U.shape[0], st), np.float32)
+            buf[:, :R] = U
+            m = _Matrix(U.shape[0], R, U.shape[0], st, buf.ctypes.data)
+            rc = self.L.ptiSparseTensorMulMatrix(C.byref(Y), C.byref(t), C.byref(m), C.c_uint32(mode))
+        assert rc == 0
+        nf, st = int(Y.nnz), int(Y.stride)
+        finds = [_np_from(Y.inds[m].data, int(Y.inds[m].len), np.uint32) if Y.inds[m].len else np.empty(0, np.uint32)
+                 for m in range(len(dims))]
+        yv = _np_from(Y.values.values, nf * st, np.float32).reshape(nf, st) if nf else np.empty((0, st), np.float32)
+        after = ([k.copy() for k in keep["inds"]], keep["vals"].copy(), keep["sortorder"].copy())
+        return finds, yv, after
 
     def orderit(self, dims, inds, vals, iterations):
         """orderit(renumber=1) of the reference (src/sptensor/orderit.c:121-208),
