@@ -317,6 +317,88 @@ def run_gradcp(args):
             "ms_per_gradient": round(ms, 3), "loss": float(loss.item())}
 
 
+TTM_R = 16
+TTM_REF_NNZ = 2_000_000
+
+
+def run_ttm(args):
+    """TTM of the C2 tensor (50M Zipf nonzeros) with an R = 16 matrix along
+    every mode on the GPU (ptiB200TTM; fibers built once per mode, timed
+    apart), against the reference's ptiOmpSparseTensorMulMatrix (oracle/_ref,
+    all host threads) on a 2M-nonzero sample of the same construction."""
+    import numpy as np
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    coo, h, inds, vals, _ = make_c2(dev, SEED + 41)
+    h.free()
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 42)
+    out = {"workload": f"TTM of the C2 tensor (3-D 200000x150000x20000, 50M Zipf(1.1) nnz), R={TTM_R} FP32, "
+                       "each mode", "modes": []}
+    peak, _ = measured_peak()
+    for mode in range(3):
+        U = torch.rand((C2_DIMS[mode], TTM_R), generator=g, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        finds, Y = coo.ttm(U, mode)  # builds the fibers, then one TTM
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0
+        nfib = Y.shape[0]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            coo.ttm(U, mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        # the kernel's bytes: mode index + value per nonzero, fiber pointers,
+        # the factor once, Y written
+        algo = C2_NNZ * 8 + (nfib + 1) * 8 + C2_DIMS[mode] * TTM_R * 4 + nfib * Y.shape[1] * 4
+        out["modes"].append({"mode": mode, "fibers": int(nfib), "ms": round(ms, 3),
+                             "fiber_build_plus_first_s": round(build_s, 3),
+                             "algorithmic_GBps": round(algo / ms / 1e6, 1),
+                             "frac_of_hbm": round(algo / ms / 1e6 / peak, 3)})
+        del finds, Y, U
+    out["note"] = ("timed region: ptiB200TTMFibers (cached) + ptiB200TTM per call, through the Python API "
+                   "(allocates Y each call)")
+    coo.free()
+    try:
+        from oracle.oracle import Ref
+        ref = Ref() if Ref.available() else None
+    except Exception:
+        ref = None
+    if ref is not None:
+        sample = np.unique(np.stack([i[:TTM_REF_NNZ].cpu().numpy() for i in inds], 1), axis=0)
+        sinds = [sample[:, m].astype(np.uint32) for m in range(3)]
+        svals = np.random.default_rng(SEED + 43).random(sample.shape[0]).astype(np.float32)
+        U = np.random.default_rng(SEED + 44).random((C2_DIMS[2], TTM_R)).astype(np.float32)
+        import ctypes as C
+        from oracle.oracle import _Matrix, _SemiSparse
+        t, keep = ref._coo(C2_DIMS, sinds, svals)
+        st = ((TTM_R - 1) // 8 + 1) * 8
+        buf = np.zeros((C2_DIMS[2], st), np.float32)
+        buf[:, :TTM_R] = U
+        mtx = _Matrix(C2_DIMS[2], TTM_R, C2_DIMS[2], st, buf.ctypes.data)
+        Y = _SemiSparse()
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)
+        try:
+            t0 = time.perf_counter()
+            ref.L.ptiOmpSparseTensorMulMatrix(C.byref(Y), C.byref(t), C.byref(mtx), C.c_uint32(2))
+            ref_s = time.perf_counter() - t0
+        finally:
+            os.dup2(saved, 1)
+            os.close(devnull)
+            os.close(saved)
+        out["reference_cpu"] = {"kind": "reference", "cores": os.cpu_count(), "mode": 2,
+                                "sample": f"{sample.shape[0]} unique nonzeros of the same construction, "
+                                          "ptiOmpSparseTensorMulMatrix incl. its sort and fiber build",
+                                "s": round(ref_s, 3), "Mnnz_per_s": round(sample.shape[0] / ref_s / 1e6, 2)}
+    return out
+
+
 RENUM_REF_NNZ = 200_000
 
 
@@ -828,7 +910,8 @@ def main():
     ap.add_argument("--batched-iters", type=int, default=C5_ITERS)
     ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
     ap.add_argument("--no-renumber", action="store_true", help="skip the renumbering block")
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber"], default=None,
+    ap.add_argument("--no-ttm", action="store_true", help="skip the TTM block")
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm"], default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
                     help="C5 tensors (spread over the size range) checked against the FP64 oracle")
@@ -856,7 +939,7 @@ def main():
         import torch
         torch.cuda.set_device(0)
         block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
-                 "renumber": run_renumber}[args.only]
+                 "renumber": run_renumber, "ttm": run_ttm}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
         return
     rank, world, _ = dist_setup(args.gpus)
@@ -884,6 +967,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["renumber"] = run_renumber(args)
+        if world == 1 and not args.no_ttm:
+            import torch
+            torch.cuda.empty_cache()
+            res["ttm"] = run_ttm(args)
         print(json.dumps(res), flush=True)
     from hiparti_b200 import replicas
     replicas.shutdown(world)

@@ -51,6 +51,8 @@ struct FiberPlan {
     DevBuf sind;                           // uint32 [nnz]: the mode's index, fiber order
     DevBuf sval;                           // float  [nnz]: values, fiber order
     DevBuf perm;                           // uint32 [nnz]: fiber-order position -> input nonzero
+    uint64_t nlong = 0;                    // fibers longer than the one-thread-per-fiber limit
+    DevBuf long_fibers;                    // uint32 [nlong]: their indices
 };
 
 }  // namespace pti

@@ -13,12 +13,17 @@
 //
 // Here the sort is a stable LSD radix sort (the mode first, then the other
 // modes from the last to the first) and the fibers come from a scan over
-// "coordinates changed" flags; the fiber structure is kept per mode.  The TTM
-// kernel gives each fiber a group of G lanes (G = 8, 16 or 32 by R), each lane
-// CPL columns; the group loads G nonzeros of its fiber at a time and then
-// walks them in order, so every Y element is the same sequence of FP32
-// multiply-then-add steps as the reference's loop, and the result is
-// bit-identical for tensors with distinct coordinates.
+// "coordinates changed" flags; the fiber structure is kept per mode.  Two
+// kernels share the fibers, and in both every Y element is the same sequence
+// of FP32 multiply-then-add steps as the reference's loop, so the result is
+// bit-identical for tensors with distinct coordinates:
+//   - ttm_short_kernel (R <= 32): one thread per fiber of at most kShortFiber
+//     nonzeros, all R columns in registers, each factor row read as float4s.
+//     Most fibers are short, and a thread per fiber keeps many fibers' load
+//     chains in flight at once;
+//   - ttm_kernel: a group of G lanes (G = 8, 16 or 32 by R) per fiber, each
+//     lane CPL columns; the group loads G nonzeros at a time and walks them in
+//     order.  It takes the long fibers (and every fiber when R > 32).
 #include <cerrno>
 
 #include "primitives.cuh"
@@ -84,10 +89,159 @@ struct FiberOut {
 
 __global__ void set_last_t(uint64_t *fptr, uint64_t nfib, uint64_t nnz) { fptr[nfib] = nnz; }
 
+constexpr uint32_t kShortFiber = 64;  // longest fiber a single thread takes
+
+__global__ void long_fibers_k(const uint64_t *fptr, uint64_t nfib, uint32_t *list, unsigned long long *count)
+{
+    GRID_LOOP(f, nfib)
+    if (fptr[f + 1] - fptr[f] > kShortFiber) list[atomicAdd(count, 1ull)] = (uint32_t)f;
+}
+
+// One thread per short fiber, NC4 float4 column chunks (R <= 4 * NC4 <= 32).
+// U rows and Y rows are 16-byte aligned (ldu, ldy multiples of 4).
+template <int NC4>
+__global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restrict__ fptr, uint64_t nfib,
+                                                        const uint32_t *__restrict__ sind,
+                                                        const float *__restrict__ sval,
+                                                        const float *__restrict__ U, uint32_t ldu,
+                                                        float *__restrict__ Y, uint32_t ldy, uint32_t R)
+{
+    GRID_LOOP(f, nfib)
+    {
+        const uint64_t b = fptr[f], e = fptr[f + 1];
+        if (e - b > kShortFiber) continue;
+        float4 acc[NC4];
+#pragma unroll
+        for (int c = 0; c < NC4; ++c) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t r = sind[b];
+        float x = sval[b];
+        for (uint64_t j = b; j < e; ++j) {
+            // the next nonzero's index and value load while this one is added
+            const uint32_t rn = j + 1 < e ? sind[j + 1] : 0u;
+            const float xn = j + 1 < e ? sval[j + 1] : 0.f;
+            const float4 *u = reinterpret_cast<const float4 *>(U + (size_t)r * ldu);
+#pragma unroll
+            for (int c = 0; c < NC4; ++c) {
+                const float4 v = __ldg(u + c);
+                acc[c].x = __fadd_rn(acc[c].x, __fmul_rn(x, v.x));
+                acc[c].y = __fadd_rn(acc[c].y, __fmul_rn(x, v.y));
+                acc[c].z = __fadd_rn(acc[c].z, __fmul_rn(x, v.z));
+                acc[c].w = __fadd_rn(acc[c].w, __fmul_rn(x, v.w));
+            }
+            r = rn;
+            x = xn;
+        }
+        float4 *y = reinterpret_cast<float4 *>(Y + (size_t)f * ldy);
+#pragma unroll
+        for (int c = 0; c < NC4; ++c) {
+            float4 v = acc[c];
+            // columns at or beyond R (the U pad is not read as data): zero
+            if (4 * c + 0 >= (int)R) v.x = 0.f;
+            if (4 * c + 1 >= (int)R) v.y = 0.f;
+            if (4 * c + 2 >= (int)R) v.z = 0.f;
+            if (4 * c + 3 >= (int)R) v.w = 0.f;
+            y[c] = v;
+        }
+        for (uint32_t k = 4 * NC4; k < ldy; k += 4) y[k / 4] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// Long fibers (R <= 32, U rows 16-byte aligned): one warp per fiber, lane l
+// summing column l.  Two cp.async stages run ahead of the sums, in groups of
+// 32 nonzeros (lane t copying element t of a group):
+//   iteration g  copies the indices and values of group g + D into rings,
+//                copies the factor rows of group g (the indices landed D
+//                iterations ago) into the row ring,
+//                sums group g - D (its rows landed),
+// so 32 D rows are in flight per fiber while every column is summed in the
+// reference's order.  One cp.async.wait_group D-1 at the top of each
+// iteration covers both stages: everything committed at iteration g - D or
+// earlier has landed.  Dynamic shared memory: row ring (D+1) x 32 x W floats
+// (W = R rounded up to 4), index and value rings 2D+2 slots of 32.
+constexpr int kLongD = 12;
+constexpr int kLongRowSlots = kLongD + 1;
+constexpr int kLongIdxSlots = 2 * kLongD + 2;
+
+inline size_t long_smem_bytes(uint32_t W)
+{
+    return (size_t)kLongRowSlots * 32 * W * 4 + (size_t)kLongIdxSlots * 32 * 8;
+}
+
+__global__ void __launch_bounds__(32) ttm_long_kernel(const uint64_t *__restrict__ fptr,
+                                                      const uint32_t *__restrict__ list, uint64_t nlong,
+                                                      const uint32_t *__restrict__ sind,
+                                                      const float *__restrict__ sval, const float *__restrict__ U,
+                                                      uint32_t ldu, uint32_t R, uint32_t W, float *__restrict__ Y,
+                                                      uint32_t ldy)
+{
+    extern __shared__ __align__(16) float ring[];
+    float *su = ring;                                                    // [slot][32][W]
+    uint32_t *si = reinterpret_cast<uint32_t *>(su + (size_t)kLongRowSlots * 32 * W);  // [slot][32]
+    float *sx = reinterpret_cast<float *>(si + kLongIdxSlots * 32);      // [slot][32]
+    const int lane = threadIdx.x;
+    auto cp4 = [](void *dst, const void *src) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    };
+    for (uint64_t i = blockIdx.x; i < nlong; i += gridDim.x) {
+        const uint64_t f = list[i];
+        const uint64_t b = fptr[f], e = fptr[f + 1];
+        const int64_t ng = (int64_t)((e - b + 31) / 32);
+        float acc = 0.f;
+        for (int64_t g = -kLongD; g < ng + kLongD; ++g) {
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(kLongD - 1) : "memory");
+            __syncwarp();
+            const int64_t gc = g - kLongD;  // group summed now
+            if (gc >= 0) {
+                const uint64_t j0 = b + 32 * (uint64_t)gc;
+                const int cnt = (e - j0) < 32 ? (int)(e - j0) : 32;
+                const float *rows = su + (size_t)(gc % kLongRowSlots) * 32 * W;
+                const float *xs = sx + (gc % kLongIdxSlots) * 32;
+                if ((uint32_t)lane < R) {
+#pragma unroll 8
+                    for (int t = 0; t < cnt; ++t) acc = __fadd_rn(acc, __fmul_rn(xs[t], rows[(size_t)t * W + lane]));
+                }
+            }
+            if (g >= 0 && g < ng) {  // rows of group g
+                const uint64_t mine = b + 32 * (uint64_t)g + lane;
+                if (mine < e) {
+                    const uint32_t r = si[(g % kLongIdxSlots) * 32 + lane];  // this lane's own copy
+                    const float *src = U + (size_t)r * ldu;
+                    float *dst = su + (size_t)(g % kLongRowSlots) * 32 * W + (size_t)lane * W;
+                    for (uint32_t q = 0; q < W; q += 4) {
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+                                     ::"r"((unsigned)__cvta_generic_to_shared(dst + q)), "l"(src + q)
+                                     : "memory");
+                    }
+                }
+            }
+            const int64_t gi = g + kLongD;  // indices and values of group gi
+            if (gi >= 0 && gi < ng) {
+                const uint64_t mine = b + 32 * (uint64_t)gi + lane;
+                if (mine < e) {
+                    const int slot = (int)(gi % kLongIdxSlots) * 32 + lane;
+                    cp4(si + slot, sind + mine);
+                    cp4(sx + slot, sval + mine);
+                }
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            __syncwarp();  // the slots read above are refilled in later iterations
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        float *y = Y + (size_t)f * ldy;
+        if ((uint32_t)lane < R) y[lane] = acc;
+        for (uint32_t k = R + lane; k < ldy; k += 32) y[k] = 0.f;
+        __syncwarp();
+    }
+}
+
 // One group of G lanes per fiber; lane l of the group owns columns
 // l, l + G, ..., l + (CPL-1) G.  Pad columns [R, ldy) are written as zero.
+// With `list`, the groups take the fibers list[0 .. nfib) instead of 0 .. nfib.
 template <int CPL>
 __global__ void __launch_bounds__(256) ttm_kernel(const uint64_t *__restrict__ fptr, uint64_t nfib,
+                                                  const uint32_t *__restrict__ list,
                                                   const uint32_t *__restrict__ sind,
                                                   const float *__restrict__ sval, const float *__restrict__ U,
                                                   uint32_t ldu, uint32_t R, float *__restrict__ Y, uint32_t ldy,
@@ -98,7 +252,8 @@ __global__ void __launch_bounds__(256) ttm_kernel(const uint64_t *__restrict__ f
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane - gl);
     const uint64_t groups = (uint64_t)gridDim.x * (blockDim.x / G);
     const uint64_t g0 = (uint64_t)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
-    for (uint64_t f = g0; f < nfib; f += groups) {
+    for (uint64_t i = g0; i < nfib; i += groups) {
+        const uint64_t f = list ? list[i] : i;
         float acc[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
@@ -229,8 +384,22 @@ int fiber_plan(ptiB200Tensor *t, uint32_t mode, bool sort, cudaStream_t s)
         PTI_TRY((exclusive_scan<uint64_t>(FiberHeadIn{a}, FiberOut{a}, n, tmp.as<uint64_t>(), &nfib, s)));
     }
     set_last_t<<<1, 1, 0, s>>>(P.fptr.as<uint64_t>(), nfib, n);
+    // fibers too long for one thread each (their order in the list is free:
+    // every fiber is computed on its own)
+    DevBuf cnt;
+    PTI_CUDA(cnt.alloc(padded(8), s), mod);
+    PTI_CUDA(cudaMemsetAsync(cnt.ptr, 0, 8, s), mod);
+    PTI_CUDA(P.long_fibers.alloc(padded(nfib * 4), s), mod);
+    unsigned long long nlong = 0;
+    if (nfib) {
+        long_fibers_k<<<grid_t(nfib), 256, 0, s>>>(P.fptr.as<uint64_t>(), nfib, P.long_fibers.as<uint32_t>(),
+                                                  cnt.as<unsigned long long>());
+        PTI_CUDA(cudaMemcpyAsync(&nlong, cnt.ptr, 8, cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+    }
     PTI_CUDA(cudaGetLastError(), mod);
     P.nfib = nfib;
+    P.nlong = nlong;
     P.ready = true;
     return 0;
 }
@@ -252,19 +421,66 @@ int ttm_device(ptiB200Tensor *t, uint32_t mode, const float *U, uint32_t R, uint
         return 0;
     }
     PTI_CHECK(R >= 1 && R <= 256 && ldu >= R && ldy >= R, PTIERR_VALUE_ERROR, mod, "rank must be in [1, 256]");
-    const int G = R > 16 ? 32 : (R > 8 ? 16 : 8);
-    const int cpl = (int)((R + G - 1) / G);
-    const uint64_t groups_needed = P.nfib;
-    const unsigned per_cta = 256 / G;
-    const unsigned grid =
-        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups_needed + per_cta - 1) / per_cta, (uint64_t)sms * 16));
     const uint64_t *fp = P.fptr.as<uint64_t>();
     const uint32_t *si = P.sind.as<uint32_t>();
     const float *sv = P.sval.as<float>();
-    if (cpl <= 1) ttm_kernel<1><<<grid, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, R, Y, ldy, G);
-    else if (cpl <= 2) ttm_kernel<2><<<grid, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, R, Y, ldy, G);
-    else if (cpl <= 4) ttm_kernel<4><<<grid, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, R, Y, ldy, G);
-    else ttm_kernel<8><<<grid, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, R, Y, ldy, G);
+    const uint32_t nc4 = (R + 3) / 4;
+    // thread per short fiber: R <= 32, float4 rows (ldu, ldy multiples of 4
+    // and at least 4 * nc4, both arrays 16-byte aligned)
+    const bool short_path = R <= 32 && ldu % 4 == 0 && ldy % 4 == 0 && ldu >= 4 * nc4 && ldy >= 4 * nc4 &&
+                            reinterpret_cast<uintptr_t>(U) % 16 == 0 && reinterpret_cast<uintptr_t>(Y) % 16 == 0;
+    uint64_t ngroup = P.nfib;
+    const uint32_t *list = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool joined = true;
+    if (short_path && P.nlong) {
+        // the long fibers run beside the short ones, on a second stream
+        const uint32_t W = 4 * nc4;
+        const size_t smem = long_smem_bytes(W);
+        PTI_CUDA(cudaFuncSetAttribute(ttm_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 mod);
+        cudaStream_t s2 = copy_stream();
+        PTI_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), mod);
+        PTI_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), mod);
+        PTI_CUDA(cudaEventRecord(ev[0], s), mod);
+        PTI_CUDA(cudaStreamWaitEvent(s2, ev[0], 0), mod);
+        const unsigned grid = (unsigned)std::min<uint64_t>(P.nlong, (uint64_t)sms * 8);
+        ttm_long_kernel<<<grid, 32, smem, s2>>>(fp, P.long_fibers.as<uint32_t>(), P.nlong, si, sv, U, ldu, R, W, Y,
+                                                ldy);
+        PTI_CUDA(cudaGetLastError(), mod);
+        PTI_CUDA(cudaEventRecord(ev[1], s2), mod);
+        joined = false;
+    }
+    if (short_path) {
+        const unsigned g = grid_t(P.nfib);
+        switch (nc4) {
+        case 1: ttm_short_kernel<1><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 2: ttm_short_kernel<2><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 3: ttm_short_kernel<3><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 4: ttm_short_kernel<4><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 5: ttm_short_kernel<5><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 6: ttm_short_kernel<6><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        case 7: ttm_short_kernel<7><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        default: ttm_short_kernel<8><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        }
+        ngroup = 0;  // the long fibers are on the second stream
+    }
+    if (!joined) {  // `s` continues once the long fibers are done too
+        PTI_CUDA(cudaStreamWaitEvent(s, ev[1], 0), mod);
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    }
+    if (ngroup) {
+        const int G = R > 16 ? 32 : (R > 8 ? 16 : 8);
+        const int cpl = (int)((R + G - 1) / G);
+        const unsigned per_cta = 256 / G;
+        const unsigned grid =
+            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ngroup + per_cta - 1) / per_cta, (uint64_t)sms * 16));
+        if (cpl <= 1) ttm_kernel<1><<<grid, 256, 0, s>>>(fp, ngroup, list, si, sv, U, ldu, R, Y, ldy, G);
+        else if (cpl <= 2) ttm_kernel<2><<<grid, 256, 0, s>>>(fp, ngroup, list, si, sv, U, ldu, R, Y, ldy, G);
+        else if (cpl <= 4) ttm_kernel<4><<<grid, 256, 0, s>>>(fp, ngroup, list, si, sv, U, ldu, R, Y, ldy, G);
+        else ttm_kernel<8><<<grid, 256, 0, s>>>(fp, ngroup, list, si, sv, U, ldu, R, Y, ldy, G);
+    }
     PTI_CUDA(cudaGetLastError(), mod);
     return 0;
 }
