@@ -885,6 +885,119 @@ def run_reference_arm(args, rank, world):
             "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+C1_DIMS = (1000, 1000, 1000)
+C1_NNZ = 1_000_000
+C1_R = 16
+CPD_SAMPLE_NNZ = 2_000_000
+
+
+def run_cpu_paths(args):
+    """The reference's other CPU paths beside ours on the same bounded inputs
+    (rank 0, N = 1): COO->HiCOO conversion of the 4M-nonzero C2 sample
+    (ptiSparseTensorToHiCOO(tk=1) against the GPU conversion), the C1 COO
+    MTTKRP (ptiOmpMTTKRP with atomics and ptiOmpMTTKRP_Reduce against the
+    device COO kernel), and CPD-ALS iterations on a 2M-nonzero sample of the
+    C3 construction (OmpCpdAlsStep against ptiB200CpdAls, R = 32)."""
+    import numpy as np
+    import torch
+    from oracle.oracle import Ref
+    from hiparti_b200 import COOTensor, DeviceTensor
+    from hiparti_b200.synth import coords_numpy, planted_tensor
+    if not Ref.available():
+        return {"unavailable": "reference library oracle/_ref not built"}
+    ref = Ref()
+    threads = os.cpu_count() or 1
+    out = {"threads": threads}
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    # conversion
+    inds = coords_numpy(C2_DIMS, args.ref_sample, SEED, zipf_s=1.1)
+    vals = np.random.default_rng(SEED + 1).random(args.ref_sample, dtype=np.float32)
+    t0 = time.perf_counter()
+    ref.to_hicoo(list(C2_DIMS), inds, vals, C2_SB, C2_SK, C2_SC)
+    ref_conv = time.perf_counter() - t0
+    coo = DeviceTensor.from_coo(COOTensor(C2_DIMS, inds, vals))
+    h = coo.to_hicoo(C2_SB, C2_SK, C2_SC)  # warm-up
+    h.free()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h = coo.to_hicoo(C2_SB, C2_SK, C2_SC)
+    torch.cuda.synchronize()
+    ours_conv = time.perf_counter() - t0
+    h.free()
+    coo.free()
+    out["conversion"] = {"sample_nnz": args.ref_sample, "s_reference_tk1": round(ref_conv, 3),
+                         "s_ours_gpu_device_resident": round(ours_conv, 4), "speedup": round(ref_conv / ours_conv, 1)}
+
+    # C1 COO MTTKRP, 3 modes
+    inds = coords_numpy(C1_DIMS, C1_NNZ, SEED + 51)
+    vals = np.random.default_rng(SEED + 52).random(C1_NNZ, dtype=np.float32)
+    stride = ((C1_R - 1) // 8 + 1) * 8
+    mats = [np.random.default_rng(SEED + 53 + m).random((d, stride), dtype=np.float32) for m, d in enumerate(C1_DIMS)]
+    step_bytes = 3 * (C1_NNZ * (3 * 4 + 4) + 4 * C1_R * sum(C1_DIMS))
+    res = {}
+    for variant in ("omp", "omp_reduce"):
+        for m in range(3):  # warm-up
+            ref.mttkrp_coo(list(C1_DIMS), inds, vals, mats, C1_R, m, variant=variant, tk=threads)
+        t0 = time.perf_counter()
+        for m in range(3):
+            ref.mttkrp_coo(list(C1_DIMS), inds, vals, mats, C1_R, m, variant=variant, tk=threads)
+        res[variant] = time.perf_counter() - t0
+    dt = DeviceTensor.from_coo(COOTensor(C1_DIMS, inds, vals))
+    facs = [torch.from_numpy(a).to(dev) for a in mats]
+    for m in range(3):
+        dt.prepare(m)
+        dt.mttkrp(facs, m, rank=C1_R)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        for m in range(3):
+            dt.mttkrp(facs, m, rank=C1_R)
+    e1.record()
+    torch.cuda.synchronize()
+    ours_ms = e0.elapsed_time(e1) / 10
+    dt.free()
+    out["coo_mttkrp_c1"] = {"workload": "C1: 3-D 1000^3, 1M uniform nnz, R=16, 3 modes per step",
+                            "GBps_reference_omp_atomic": round(step_bytes / res["omp"] / 1e9, 3),
+                            "GBps_reference_omp_reduce": round(step_bytes / res["omp_reduce"] / 1e9, 3),
+                            "GBps_ours_device": round(step_bytes / ours_ms / 1e6, 1),
+                            "ms_ours_per_step": round(ours_ms, 4)}
+
+    # CPD iterations on a C3-construction sample
+    dims = C3_DIMS
+    inds, vals, _ = planted_tensor(dims, CPD_SAMPLE_NNZ, 10, 0.01, seed=SEED + 61)
+    R = C3_R
+    rng = np.random.default_rng(SEED + 62)
+    init = [rng.random((d, R)).astype(np.float32) for d in dims]
+    iters = 3
+    t0 = time.perf_counter()
+    ref.cpd_als_step(list(dims), inds, vals, R, iters, init, tk=threads)
+    ref_iter = (time.perf_counter() - t0) / iters
+    dtc = DeviceTensor.from_hicoo(COOTensor(dims, inds, vals).to_hicoo(C2_SB, C2_SK, C2_SC))
+    stride = ((R - 1) // 8 + 1) * 8
+
+    def dev_factors():
+        fs = []
+        for a in init:
+            f = torch.zeros((a.shape[0], stride), dtype=torch.float32)
+            f[:, :R] = torch.from_numpy(a)
+            fs.append(f.to(dev))
+        return fs
+    dtc.cpd_als(dev_factors(), 2, rank=R)  # warm-up (schedules)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dtc.cpd_als(dev_factors(), 10, rank=R)
+    torch.cuda.synchronize()
+    ours_iter = (time.perf_counter() - t0) / 10
+    dtc.free()
+    out["cpd_c3_sample"] = {"workload": f"C3 construction, {CPD_SAMPLE_NNZ} nnz, R={R}",
+                            "s_per_iter_reference_OmpCpdAlsStep": round(ref_iter, 4),
+                            "s_per_iter_ours_hicoo_fp32": round(ours_iter, 5),
+                            "speedup": round(ref_iter / ours_iter, 1)}
+    return out
+
+
 def cpu_baseline_block(args):
     """Reference OpenMP HiCOO MTTKRP on a bounded sample (rank 0, N=1)."""
     res = run_reference_arm(argparse.Namespace(warmup=0, steps=1, ref_sample=args.ref_sample), 0, 1)
@@ -911,7 +1024,8 @@ def main():
     ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
     ap.add_argument("--no-renumber", action="store_true", help="skip the renumbering block")
     ap.add_argument("--no-ttm", action="store_true", help="skip the TTM block")
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm"], default=None,
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm", "cpu_paths"],
+                    default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
                     help="C5 tensors (spread over the size range) checked against the FP64 oracle")
@@ -939,7 +1053,7 @@ def main():
         import torch
         torch.cuda.set_device(0)
         block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
-                 "renumber": run_renumber, "ttm": run_ttm}[args.only]
+                 "renumber": run_renumber, "ttm": run_ttm, "cpu_paths": run_cpu_paths}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
         return
     rank, world, _ = dist_setup(args.gpus)
@@ -947,6 +1061,7 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_block(args)
+            res["reference_cpu_paths"] = run_cpu_paths(args)
         if world == 1 and not args.no_cpd:
             import torch
             torch.cuda.empty_cache()
