@@ -280,12 +280,20 @@ struct HiSmem {
     static constexpr uint32_t blk = ein + NIN * kHiTile;                // u16[kHiTile]
     static constexpr uint32_t brow = blk + 2 * kHiTile;                 // u32[kHiTile + 4]
     static constexpr uint32_t bin = brow + 4 * (kHiTile + 4);           // u32[NIN][kHiTile + 4]
-    static constexpr uint32_t slots = bin + 4 * NIN * (kHiTile + 4);    // float[kSchedThreads * CPL]
-    static constexpr uint32_t total = slots + 4 * kSchedThreads * CPL;
+    static constexpr uint32_t staged = bin + 4 * NIN * (kHiTile + 4);   // end of the staged tile
     // decoded records, written over the staged arrays once they are read
     static constexpr uint32_t rec = 0;                                  // uint4[kHiTile]
     static constexpr uint32_t rval = rec + 16 * kHiTile;                // float[kHiTile] (4-D only)
-    static_assert(rval + (NIN == 3 ? 4 * kHiTile : 0) <= slots, "records must fit over the staged tile");
+    // FP32 rows (CPL 4): the groups' merge slots follow the records, over
+    // the staged tile (they are first written during the walk, after the
+    // decode), which lets one more CTA share an SM.  BF16 rows (CPL 8) keep
+    // them after the tile: their walk is bound by L1 wavefronts, and the
+    // extra CTA's shared memory comes out of the L1 that caches the rows.
+    static constexpr uint32_t slots =
+        CPL == 4 ? rval + (NIN == 3 ? 4 * kHiTile : 0) : staged;  // float[kSchedThreads * CPL]
+    static constexpr uint32_t slots_end = slots + 4 * kSchedThreads * CPL;
+    static constexpr uint32_t total = staged > slots_end ? staged : slots_end;
+    static_assert(slots <= staged, "records must fit over the staged tile");
 };
 
 // HiCOO schedule, one CTA per tile of kHiTile nonzeros.  The tile's nonzeros
