@@ -584,6 +584,29 @@ int ptiOmpMTTKRP_Reduce(ptiSparseTensor const *const X, ptiMatrix *mats[], ptiMa
     (void)tk;
     return pti::mttkrp_host_coo(X, mats, mats_order, mode);
 }
+struct ptiMutexPool {
+    uint32_t nlocks, padsize;  // recorded only: the GPU path takes no locks
+};
+ptiMutexPool *SptMutexAllocCustom(ptiIndex const num_locks, ptiIndex const pad_size)
+{
+    auto *p = static_cast<ptiMutexPool *>(std::malloc(sizeof(ptiMutexPool)));
+    if (p) {
+        p->nlocks = num_locks;
+        p->padsize = pad_size;
+    }
+    return p;
+}
+ptiMutexPool *ptiMutexAlloc(void) { return SptMutexAllocCustom(1024, 16); }
+void ptiMutexFree(ptiMutexPool *pool) { std::free(pool); }
+
+int ptiOmpMTTKRP_Lock(ptiSparseTensor const *const X, ptiMatrix *mats[], ptiIndex const mats_order[],
+                      ptiIndex const mode, const int tk, ptiMutexPool *lock_pool)
+{
+    (void)tk;
+    (void)lock_pool;
+    return pti::mttkrp_host_coo(X, mats, mats_order, mode);
+}
+
 int ptiCudaMTTKRP(ptiSparseTensor const *const X, ptiMatrix *mats[], ptiIndex *const mats_order,
                   ptiIndex const mode, ptiIndex const impl_num)
 {
@@ -608,6 +631,71 @@ int ptiOmpMTTKRPHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiMatrix *mats[]
     (void)tb;
     return pti::mttkrp_host_hicoo(hitsr, mats, mats_order, mode);
 }
+// ptiRankMatrix (8-bit ncols and stride) viewed as ptiMatrix for the shared
+// MTTKRP path; the values are shared, so the result lands in mats[N] itself.
+static int mttkrp_rank_hicoo(ptiSparseTensorHiCOO const *const hitsr, ptiRankMatrix *mats[],
+                             ptiIndex const mats_order[], ptiIndex const mode)
+{
+    const char *mod = "B200 HiSpTns MTTKRP";
+    PTI_CHECK(hitsr && mats, PTIERR_VALUE_ERROR, mod, "null argument");
+    const uint32_t N = hitsr->nmodes;
+    PTI_CHECK(N >= 2 && N <= (uint32_t)pti::kMaxModes, PTIERR_VALUE_ERROR, mod, "unsupported number of modes");
+    ptiMatrix views[pti::kMaxModes + 1];
+    ptiMatrix *ptrs[pti::kMaxModes + 1];
+    for (uint32_t m = 0; m <= N; ++m) {
+        PTI_CHECK(mats[m], PTIERR_VALUE_ERROR, mod, "null matrix");
+        views[m].nrows = mats[m]->nrows;
+        views[m].ncols = mats[m]->ncols;
+        views[m].cap = mats[m]->cap;
+        views[m].stride = mats[m]->stride;
+        views[m].values = mats[m]->values;
+        ptrs[m] = &views[m];
+    }
+    return pti::mttkrp_host_hicoo(hitsr, ptrs, mats_order, mode);
+}
+
+int ptiMTTKRPHiCOO_MatrixTiling(ptiSparseTensorHiCOO const *const hitsr, ptiRankMatrix *mats[],
+                                ptiIndex const mats_order[], ptiIndex const mode)
+{
+    return mttkrp_rank_hicoo(hitsr, mats, mats_order, mode);
+}
+int ptiOmpMTTKRPHiCOO_MatrixTiling(ptiSparseTensorHiCOO const *const hitsr, ptiRankMatrix *mats[],
+                                   ptiIndex const mats_order[], ptiIndex const mode, const int tk, const int tb)
+{
+    (void)tk;
+    (void)tb;
+    return mttkrp_rank_hicoo(hitsr, mats, mats_order, mode);
+}
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled(ptiSparseTensorHiCOO const *const hitsr, ptiRankMatrix *mats[],
+                                             ptiIndex const mats_order[], ptiIndex const mode, const int tk,
+                                             const int tb, int balanced)
+{
+    (void)tk;
+    (void)tb;
+    (void)balanced;
+    return mttkrp_rank_hicoo(hitsr, mats, mats_order, mode);
+}
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce(ptiSparseTensorHiCOO const *const hitsr, ptiRankMatrix *mats[],
+                                                    ptiRankMatrix *copy_mats[], ptiIndex const mats_order[],
+                                                    ptiIndex const mode, const int tk, const int tb, int balanced)
+{
+    (void)copy_mats;
+    (void)tk;
+    (void)tb;
+    (void)balanced;
+    return mttkrp_rank_hicoo(hitsr, mats, mats_order, mode);
+}
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce_Two(ptiSparseTensorHiCOO const *const hitsr,
+                                                        ptiRankMatrix *mats[], ptiRankMatrix *copy_mats[],
+                                                        ptiIndex const mats_order[], ptiIndex const mode,
+                                                        const int tk, const int tb)
+{
+    (void)copy_mats;
+    (void)tk;
+    (void)tb;
+    return mttkrp_rank_hicoo(hitsr, mats, mats_order, mode);
+}
+
 int ptiCudaMTTKRPHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiMatrix **const mats, ptiIndex *const mats_order,
                        ptiIndex const mode, ptiNnzIndex const max_nnzb, int const impl_num)
 {

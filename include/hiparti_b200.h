@@ -265,6 +265,15 @@ int ptiOmpMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex c
 /* include/includes/sptensors.h:190-196 (copy_mats unused; tk ignored) */
 int ptiOmpMTTKRP_Reduce(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiMatrix * copy_mats[],
                         ptiIndex const mats_order[], ptiIndex const mode, const int tk);
+/* include/includes/sptensors.h:197-203 (lock_pool accepted and unused: the GPU
+ * path privatises rows instead of locking) and the OpenMP lock pool of
+ * include/includes/helper_funcs.h:61-65 (opaque here). */
+typedef struct ptiMutexPool ptiMutexPool;
+ptiMutexPool * ptiMutexAlloc(void);
+ptiMutexPool * SptMutexAllocCustom(ptiIndex const num_locks, ptiIndex const pad_size);
+void ptiMutexFree(ptiMutexPool * pool);
+int ptiOmpMTTKRP_Lock(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex const mats_order[],
+                      ptiIndex const mode, const int tk, ptiMutexPool * lock_pool);
 /* include/includes/sptensors.h:204-215, src/sptensor/mttkrp_cuda.cu:41-374 and
  * src/sptensor/mttkrp_cuda_onekernel.cu:41-426 (impl_num ignored; any order N). */
 int ptiCudaMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex * const mats_order,
@@ -280,6 +289,24 @@ int ptiOmpMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix * mats
                       ptiIndex const mats_order[], ptiIndex const mode, const int tk, const int tb);
 /* include/includes/sptensors.h:302-308, src/sptensor/hicoo/mttkrp_cuda.cu:41-265
  * (max_nnzb and impl_num ignored: no limit on nonzeros per block; any order N). */
+/* include/includes/sptensors.h:258-300, src/sptensor/hicoo/mttkrp.c:313-404 and
+ * hicoo/mttkrp_omp.c: the same MTTKRP with ptiRankMatrix factors (8-bit ncols and
+ * stride).  tk, tb, balanced and copy_mats are accepted and unused. */
+int ptiMTTKRPHiCOO_MatrixTiling(ptiSparseTensorHiCOO const * const hitsr, ptiRankMatrix * mats[],
+                                ptiIndex const mats_order[], ptiIndex const mode);
+int ptiOmpMTTKRPHiCOO_MatrixTiling(ptiSparseTensorHiCOO const * const hitsr, ptiRankMatrix * mats[],
+                                   ptiIndex const mats_order[], ptiIndex const mode, const int tk, const int tb);
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled(ptiSparseTensorHiCOO const * const hitsr, ptiRankMatrix * mats[],
+                                             ptiIndex const mats_order[], ptiIndex const mode, const int tk,
+                                             const int tb, int balanced);
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce(ptiSparseTensorHiCOO const * const hitsr,
+                                                    ptiRankMatrix * mats[], ptiRankMatrix * copy_mats[],
+                                                    ptiIndex const mats_order[], ptiIndex const mode,
+                                                    const int tk, const int tb, int balanced);
+int ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce_Two(ptiSparseTensorHiCOO const * const hitsr,
+                                                        ptiRankMatrix * mats[], ptiRankMatrix * copy_mats[],
+                                                        ptiIndex const mats_order[], ptiIndex const mode,
+                                                        const int tk, const int tb);
 int ptiCudaMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix ** const mats,
                        ptiIndex * const mats_order, ptiIndex const mode, ptiNnzIndex const max_nnzb,
                        int const impl_num);

@@ -471,6 +471,21 @@ class Ref:
         assert rc == 0
         return out[: dims[mode]].copy()
 
+    def mttkrp_hicoo_rank(self, dims, h, mats, R, mode):
+        """ptiMTTKRPHiCOO_MatrixTiling (ptiRankMatrix factors) of the reference."""
+        N = len(h["binds"])
+        hs, keep = self._hicoo_struct(h, dims)
+        stride = mats[0].shape[1]
+        fac = [np.ascontiguousarray(m, np.float32) for m in mats]
+        out = np.zeros((max(dims), stride), np.float32)
+        ms = [_RankMatrix(a.shape[0], R, a.shape[0], stride, a.ctypes.data) for a in fac + [out]]
+        ms[-1].nrows = dims[mode]
+        arr = (C.POINTER(_RankMatrix) * len(ms))(*[C.pointer(m) for m in ms])
+        order = np.asarray([(mode + i) % N for i in range(N)], np.uint32)
+        rc = self.L.ptiMTTKRPHiCOO_MatrixTiling(C.byref(hs), arr, _u32p(order), C.c_uint32(mode))
+        assert rc == 0
+        return out[: dims[mode]].copy()
+
     def cpd_als_step(self, dims, inds, vals, R, niters, init_mats, tk=0):
         """CpdAlsStep (tk=0) or OmpCpdAlsStep(tk, use_reduce=0) from the given
         FP32 factors with tol=0.  Returns (fit, lambda, factors)."""

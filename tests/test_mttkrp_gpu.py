@@ -168,3 +168,66 @@ def test_device_api_torch(lib, cuda, orc, fmt, dtype):
         ref = orc.mttkrp_coo(inds, vals, ref_mats, R, m)[: dims[m]]
         assert rel_err(out.cpu().numpy(), ref) < TOL
     dt.free()
+
+
+@pytest.mark.parametrize("R", [10, 32])
+def test_rank_matrix_entry_points_match_reference(lib, cuda, ref, R):
+    """ptiMTTKRPHiCOO_MatrixTiling and the OpenMP MatrixTiling variants
+    (ptiRankMatrix factors, 8-bit ncols and stride) against the reference's
+    ptiMTTKRPHiCOO_MatrixTiling (src/sptensor/hicoo/mttkrp.c:313-542)."""
+    from hiparti_b200 import ffi
+    dims = (700, 500, 300)
+    inds, vals = synth.zipf_tensor(dims, 30000, s=1.1, seed=R)
+    mats = synth.factor_matrices(dims, R, seed=R + 3)
+    h = ref.to_hicoo(list(dims), inds, vals, 4, 9, 10)
+    ht = HiCOOTensor(dims, 4, 9, 10, h["bptr"], h["binds"], h["einds"], h["vals"], kptr=h["kptr"])
+    stride = mats[0].shape[1]
+    for mode in range(3):
+        want = ref.mttkrp_hicoo_rank(list(dims), h, mats, R, mode)
+        for variant in ("seq", "omp", "sched", "reduce", "two"):
+            out = np.full((dims[mode], stride), np.nan, np.float32)
+            keep = [np.ascontiguousarray(m) for m in mats] + [out]
+            rms = [ffi.new("ptiRankMatrix *") for _ in keep]
+            for r, a in zip(rms, keep):
+                r.nrows, r.ncols, r.cap, r.stride = a.shape[0], R, a.shape[0], stride
+                r.values = ffi.cast("ptiValue *", a.ctypes.data)
+            arr = ffi.new("ptiRankMatrix *[]", rms)
+            order = ffi.new("ptiIndex[]", [(mode + i) % 3 for i in range(3)])
+            L = lib
+            rc = {"seq": lambda: L.ptiMTTKRPHiCOO_MatrixTiling(ht.c, arr, order, mode),
+                  "omp": lambda: L.ptiOmpMTTKRPHiCOO_MatrixTiling(ht.c, arr, order, mode, 8, 1),
+                  "sched": lambda: L.ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled(ht.c, arr, order, mode, 8, 1, 0),
+                  "reduce": lambda: L.ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce(ht.c, arr, ffi.NULL, order,
+                                                                                      mode, 8, 1, 1),
+                  "two": lambda: L.ptiOmpMTTKRPHiCOO_MatrixTiling_Scheduled_Reduce_Two(ht.c, arr, ffi.NULL, order,
+                                                                                       mode, 8, 1)}[variant]()
+            assert rc == 0
+            err = float(np.abs(out[:, :R] - want[:, :R]).max() / max(np.abs(want[:, :R]).max(), 1e-30))
+            assert err < 1e-5, (mode, variant, err)
+            assert not out[:, R:].any()
+
+
+def test_lock_variant_and_mutex_pool(lib, cuda, orc):
+    """ptiOmpMTTKRP_Lock with a pool from ptiMutexAlloc gives the COO MTTKRP."""
+    from hiparti_b200 import ffi
+    dims = (60, 50, 40)
+    inds, vals = synth.uniform_tensor(dims, 5000, seed=4)
+    R = 16
+    mats = synth.factor_matrices(dims, R, seed=5)
+    coo = COOTensor(dims, inds, vals)
+    stride = mats[0].shape[1]
+    pool = lib.ptiMutexAlloc()
+    assert pool != ffi.NULL
+    for mode in range(3):
+        out = np.zeros((dims[mode], stride), np.float32)
+        keep = [np.ascontiguousarray(m) for m in mats] + [out]
+        ms = [ffi.new("ptiMatrix *") for _ in keep]
+        for m, a in zip(ms, keep):
+            m.nrows, m.ncols, m.cap, m.stride = a.shape[0], R, a.shape[0], stride
+            m.values = ffi.cast("ptiValue *", a.ctypes.data)
+        arr = ffi.new("ptiMatrix *[]", ms)
+        order = ffi.new("ptiIndex[]", [(mode + i) % 3 for i in range(3)])
+        assert lib.ptiOmpMTTKRP_Lock(coo.c, arr, order, mode, 8, pool) == 0
+        want = orc.mttkrp_coo(inds, vals, mats, R, mode)[: dims[mode]]
+        assert rel_err(out[:, :R], want[:, :R]) < 1e-5
+    lib.ptiMutexFree(pool)
