@@ -116,8 +116,38 @@ class COOTensor:
                 if Y.inds[m].len else np.empty(0, np.uint32) for m in range(N)]
         vals = (np.frombuffer(ffi.buffer(Y.values.values, 4 * nf * st), np.float32).reshape(nf, st).copy()
                 if nf else np.empty((0, st), np.float32))
+        dims = [int(Y.ndims[m]) for m in range(N)]
+        mode = int(Y.mode)
         lib().ptiFreeSemiSparseTensor(Y)
-        return {"mode": int(Y.mode), "inds": inds, "vals": vals}
+        return {"mode": mode, "dims": dims, "inds": inds, "vals": vals}
+
+    @classmethod
+    def from_semi_sparse(cls, Y, epsilon=1e-6) -> "COOTensor":
+        """ptiSemiSparseTensorToSparseTensor of a ttm()/ttv() result: the
+        entries that are NaN, infinite or normal with |v| >= epsilon, sorted."""
+        N, mode = len(Y["dims"]), Y["mode"]
+        nf, st = Y["vals"].shape
+        keep = {"dims": np.asarray(Y["dims"], np.uint32), "vals": np.ascontiguousarray(Y["vals"], np.float32),
+                "inds": [np.ascontiguousarray(i, np.uint32) for i in Y["inds"]]}
+        y = ffi.new("ptiSemiSparseTensor *")
+        y.nmodes, y.mode, y.nnz, y.stride = N, mode, nf, st
+        y.ndims = _ptr(keep["dims"], "ptiIndex *")
+        vecs = ffi.new("ptiIndexVector[]", N)
+        for m in range(N):
+            vecs[m].len = vecs[m].cap = keep["inds"][m].size
+            vecs[m].data = _ptr(keep["inds"][m], "ptiIndex *") if keep["inds"][m].size else ffi.NULL
+        y.inds = vecs
+        y.values.nrows, y.values.ncols, y.values.cap, y.values.stride = nf, st, nf, st
+        y.values.values = _ptr(keep["vals"], "ptiValue *") if nf else ffi.NULL
+        t = ffi.new("ptiSparseTensor *")
+        check(lib().ptiSemiSparseTensorToSparseTensor(t, y, float(epsilon)), "ptiSemiSparseTensorToSparseTensor")
+        nnz = t.nnz
+        dims = [t.ndims[m] for m in range(N)]
+        inds = [np.frombuffer(ffi.buffer(t.inds[m].data, 4 * nnz), np.uint32).copy() if nnz
+                else np.empty(0, np.uint32) for m in range(N)]
+        vals = np.frombuffer(ffi.buffer(t.values.data, 4 * nnz), np.float32).copy() if nnz else np.empty(0, np.float32)
+        lib().ptiFreeSparseTensor(t)
+        return cls(dims, inds, vals)
 
     def ttm(self, U, mode):
         """ptiSparseTensorMulMatrix: returns {"mode", "inds" (fiber coordinates

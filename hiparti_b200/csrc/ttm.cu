@@ -581,10 +581,148 @@ int host_ttm(ptiSemiSparseTensor *Y, ptiSparseTensor *X, const ptiValue *Uvals, 
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Semi-sparse -> sparse (src/sptensor/fromssp.c:32-84)
+// ---------------------------------------------------------------------------
+// An entry survives if it is NaN, infinite, or a normal number outside
+// (-epsilon, epsilon); zeros and subnormals are dropped.
+__device__ __forceinline__ bool ssp_keep(float v, float eps)
+{
+    const uint32_t e = (__float_as_uint(v) >> 23) & 0xFFu;
+    if (e == 0xFFu) return true;
+    if (e == 0u) return false;
+    return !(v < eps && v > -eps);
+}
+
+struct SspArgs {
+    const float *vals;   // nfib x stride
+    uint32_t width, stride, mode, nmodes;
+    float eps;
+    const uint32_t *finds[kMaxModes];
+    uint32_t *oinds[kMaxModes];
+    float *ovals;
+};
+struct SspIn {
+    SspArgs a;
+    __device__ uint64_t operator()(uint64_t i) const
+    {
+        const uint64_t f = i / a.width, j = i - f * a.width;
+        return ssp_keep(a.vals[f * a.stride + j], a.eps) ? 1 : 0;
+    }
+};
+struct SspOut {
+    SspArgs a;
+    __device__ void operator()(uint64_t i, uint64_t prefix, uint64_t keep) const
+    {
+        if (!keep) return;
+        const uint64_t f = i / a.width, j = i - f * a.width;
+        for (uint32_t m = 0; m < a.nmodes; ++m) a.oinds[m][prefix] = m == a.mode ? (uint32_t)j : a.finds[m][f];
+        a.ovals[prefix] = a.vals[f * a.stride + j];
+    }
+};
+
+__global__ void permute_u32_t(const uint32_t *src, const uint32_t *perm, uint64_t n, uint32_t *dst)
+{
+    GRID_LOOP(i, n) dst[i] = src[perm[i]];
+}
+__global__ void permute_f32_t(const float *src, const uint32_t *perm, uint64_t n, float *dst)
+{
+    GRID_LOOP(i, n) dst[i] = src[perm[i]];
+}
+
+int ssp_to_sparse(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, float eps)
+{
+    const char *mod = "SspTns -> SpTns";
+    PTI_CHECK(dest && src, PTIERR_VALUE_ERROR, mod, "null argument");
+    const uint32_t N = src->nmodes, mode = src->mode;
+    PTI_CHECK(N >= 2 && N <= (uint32_t)kMaxModes && mode < N, PTIERR_VALUE_ERROR, mod, "bad semi-sparse tensor");
+    const uint64_t nfib = src->nnz;
+    const uint32_t width = src->ndims[mode], stride = src->stride;
+    PTI_CHECK(width <= stride, PTIERR_SHAPE_MISMATCH, mod, "stride below the dense mode's size");
+    const uint64_t cells = nfib * width;
+    PTI_CHECK(cells < 0xFFFFFFFFull, PTIERR_VALUE_ERROR, mod, "too many entries");
+    cudaStream_t s = sync_stream();
+    DevBuf dv, df[kMaxModes], oi[kMaxModes], ov, tmp;
+    PTI_CUDA(dv.alloc(padded(nfib * stride * 4), s), mod);
+    if (nfib) PTI_CUDA(cudaMemcpyAsync(dv.ptr, src->values.values, nfib * stride * 4, cudaMemcpyHostToDevice, s), mod);
+    SspArgs a{};
+    a.vals = dv.as<float>();
+    a.width = width;
+    a.stride = stride;
+    a.mode = mode;
+    a.nmodes = N;
+    a.eps = eps;
+    for (uint32_t m = 0; m < N; ++m) {
+        PTI_CUDA(oi[m].alloc(padded(cells * 4), s), mod);
+        a.oinds[m] = oi[m].as<uint32_t>();
+        if (m == mode) continue;
+        PTI_CUDA(df[m].alloc(padded(nfib * 4), s), mod);
+        if (nfib) PTI_CUDA(cudaMemcpyAsync(df[m].ptr, src->inds[m].data, nfib * 4, cudaMemcpyHostToDevice, s), mod);
+        a.finds[m] = df[m].as<uint32_t>();
+    }
+    PTI_CUDA(ov.alloc(padded(cells * 4), s), mod);
+    a.ovals = ov.as<float>();
+    uint64_t nnz = 0;
+    if (cells) {
+        PTI_CUDA(tmp.alloc(padded(scan_tmp_elems<uint64_t>(cells) * 8), s), mod);
+        PTI_TRY((exclusive_scan<uint64_t>(SspIn{a}, SspOut{a}, cells, tmp.as<uint64_t>(), &nnz, s)));
+    }
+    // ptiSparseTensorSortIndex(dest, 1, 1): lexicographic, mode 0 first
+    DevBuf perm, key, si[kMaxModes], sv;
+    RadixScratch sc;
+    if (nnz > 1) {
+        PTI_CUDA(perm.alloc(padded(nnz * 4), s), mod);
+        PTI_CUDA(key.alloc(padded(nnz * 8), s), mod);
+        PTI_TRY(sc.alloc(nnz, s));
+        iota_t<<<grid_t(nnz), 256, 0, s>>>(perm.as<uint32_t>(), nnz);
+        for (int m = (int)N - 1; m >= 0; --m) {
+            gather_key_t<<<grid_t(nnz), 256, 0, s>>>(oi[m].as<uint32_t>(), perm.as<uint32_t>(), nnz,
+                                                    key.as<uint64_t>());
+            const uint32_t d = src->ndims[m];
+            PTI_TRY(radix_sort_pairs(key, perm, nnz, ((bits_t(d ? d - 1 : 0) + 7) / 8) * 8, sc, s));
+        }
+        for (uint32_t m = 0; m < N; ++m) {
+            PTI_CUDA(si[m].alloc(padded(nnz * 4), s), mod);
+            permute_u32_t<<<grid_t(nnz), 256, 0, s>>>(oi[m].as<uint32_t>(), perm.as<uint32_t>(), nnz,
+                                                     si[m].as<uint32_t>());
+            oi[m].swap(si[m]);
+        }
+        PTI_CUDA(sv.alloc(padded(nnz * 4), s), mod);
+        permute_f32_t<<<grid_t(nnz), 256, 0, s>>>(ov.as<float>(), perm.as<uint32_t>(), nnz, sv.as<float>());
+        ov.swap(sv);
+        PTI_CUDA(cudaGetLastError(), mod);
+    }
+    PTI_TRY(ptiNewSparseTensor(dest, N, src->ndims));
+    dest->nnz = nnz;
+    for (uint32_t m = 0; m < N; ++m) {
+        std::free(dest->inds[m].data);
+        dest->inds[m].len = dest->inds[m].cap = nnz;
+        dest->inds[m].data = static_cast<ptiIndex *>(std::malloc((nnz ? nnz : 1) * sizeof(ptiIndex)));
+        PTI_CHECK(dest->inds[m].data, PTIERR_OS_ERROR + ENOMEM, mod, "out of memory");
+        if (nnz) PTI_CUDA(cudaMemcpyAsync(dest->inds[m].data, oi[m].ptr, nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+    }
+    std::free(dest->values.data);
+    dest->values.len = dest->values.cap = nnz;
+    dest->values.data = static_cast<ptiValue *>(std::malloc((nnz ? nnz : 1) * sizeof(ptiValue)));
+    PTI_CHECK(dest->values.data, PTIERR_OS_ERROR + ENOMEM, mod, "out of memory");
+    if (nnz) PTI_CUDA(cudaMemcpyAsync(dest->values.data, ov.ptr, nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
 }  // namespace
 }  // namespace pti
 
 extern "C" {
+
+// include/includes/ssptensors.h:26, src/sptensor/fromssp.c:32-84, computed on
+// the GPU.  epsilon >= 0 (the reference asserts epsilon > 0; with 0 it keeps
+// every normal, infinite and NaN entry, as a build without asserts does).
+int ptiSemiSparseTensorToSparseTensor(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, ptiValue epsilon)
+{
+    PTI_CHECK(epsilon >= 0.f, PTIERR_VALUE_ERROR, "SspTns -> SpTns", "epsilon must not be negative");
+    return pti::ssp_to_sparse(dest, src, epsilon);
+}
 
 int ptiNewSemiSparseTensor(ptiSemiSparseTensor *tsr, ptiIndex nmodes, ptiIndex mode, const ptiIndex ndims[])
 {

@@ -247,6 +247,10 @@ int ptiCudaSparseTensorMulMatrixOneKernel(ptiSemiSparseTensor *Y, ptiSparseTenso
                                           ptiNnzIndex const smen_size);
 int ptiSparseTensorMulVector(ptiSemiSparseTensor *Y, ptiSparseTensor * const X, ptiValueVector * const V,
                              ptiIndex mode);
+/* include/includes/ssptensors.h:26, src/sptensor/fromssp.c:32-84: the entries
+ * of src that are NaN, infinite or normal with |v| >= epsilon, as a sparse
+ * tensor sorted lexicographically (dest uninitialised; epsilon >= 0). */
+int ptiSemiSparseTensorToSparseTensor(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, ptiValue epsilon);
 
 /* ---------------------------------------------------------------------------
  * MTTKRP.  mats[0..N-1] are the factor matrices (row i of mats[k] is the rank-R

@@ -332,6 +332,25 @@ class Ref:
         after = ([k.copy() for k in keep["inds"]], keep["vals"].copy(), keep["sortorder"].copy())
         return finds, yv, after
 
+    def ssp_to_sparse(self, Y, epsilon):
+        """ptiSemiSparseTensorToSparseTensor of the reference on a ttm() result
+        dict (mode, dims, inds, vals).  Returns (inds, vals)."""
+        N, mode = len(Y["dims"]), Y["mode"]
+        nf, st = Y["vals"].shape
+        keep = {"dims": np.asarray(Y["dims"], np.uint32).copy(),
+                "vals": np.ascontiguousarray(Y["vals"], np.float32).copy(),
+                "inds": [np.ascontiguousarray(i, np.uint32).copy() for i in Y["inds"]]}
+        vecs = (_Vec * N)(*[_Vec(keep["inds"][m].size, keep["inds"][m].size, keep["inds"][m].ctypes.data)
+                            for m in range(N)])
+        y = _SemiSparse(N, keep["dims"].ctypes.data, mode, nf, vecs, st,
+                        _Matrix(nf, st, nf, st, keep["vals"].ctypes.data))
+        t = _SpTensor()
+        rc = self.L.ptiSemiSparseTensorToSparseTensor(C.byref(t), C.byref(y), C.c_float(epsilon))
+        assert rc == 0
+        nnz = int(t.nnz)
+        inds = [_np_from(t.inds[m].data, nnz, np.uint32) for m in range(N)]
+        return inds, _np_from(t.values.data, nnz, np.float32)
+
     def orderit(self, dims, inds, vals, iterations):
         """orderit(renumber=1) of the reference (src/sptensor/orderit.c:121-208),
         its Lexi-order driver with a correct coordinate sort."""

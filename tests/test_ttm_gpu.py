@@ -111,3 +111,24 @@ def test_device_ttm_large_against_fp64(lib, cuda):
     np.testing.assert_array_equal((finds[0].long() * dims[1] + finds[1].long()).cpu().numpy(), uk.cpu().numpy())
     err = float((Y[:, :16].double() - ref).norm() / ref.norm())
     assert err < 1e-6, err
+
+
+@pytest.mark.parametrize("eps", [1e-6, 0.5, 3.0])
+def test_semi_sparse_to_sparse_matches_reference(lib, cuda, ref, eps):
+    """ptiSemiSparseTensorToSparseTensor (src/sptensor/fromssp.c) of a TTM
+    result with zeros, NaN, infinity and small values planted, against the
+    reference's own conversion."""
+    dims = (30, 25, 20)
+    inds, vals = _tensor(dims, 3000, 11)
+    U = np.random.default_rng(12).standard_normal((20, 8)).astype(np.float32)
+    coo = COOTensor(dims, [i.copy() for i in inds], vals.copy())
+    Y = coo.ttm(U, 2)
+    v = Y["vals"]
+    v[0, 0], v[1, 1], v[2, 2], v[3, 3] = 0.0, np.nan, np.inf, 1e-40  # zero, NaN, inf, subnormal
+    v[4, :8] = 1e-7
+    want_inds, want_vals = ref.ssp_to_sparse(Y, eps)
+    got = COOTensor.from_semi_sparse(Y, eps)
+    assert got.dims == Y["dims"]
+    for a, b in zip(got.inds, want_inds):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(got.vals.view(np.uint32), want_vals.view(np.uint32))
