@@ -121,24 +121,51 @@ class COOTensor:
         lib().ptiFreeSemiSparseTensor(Y)
         return {"mode": mode, "dims": dims, "inds": inds, "vals": vals}
 
-    @classmethod
-    def from_semi_sparse(cls, Y, epsilon=1e-6) -> "COOTensor":
-        """ptiSemiSparseTensorToSparseTensor of a ttm()/ttv() result: the
-        entries that are NaN, infinite or normal with |v| >= epsilon, sorted."""
+    @staticmethod
+    def _semi_struct(Y, keep):
         N, mode = len(Y["dims"]), Y["mode"]
         nf, st = Y["vals"].shape
-        keep = {"dims": np.asarray(Y["dims"], np.uint32), "vals": np.ascontiguousarray(Y["vals"], np.float32),
-                "inds": [np.ascontiguousarray(i, np.uint32) for i in Y["inds"]]}
+        keep["dims"] = np.asarray(Y["dims"], np.uint32)
+        keep["vals"] = np.ascontiguousarray(Y["vals"], np.float32)
+        keep["inds"] = [np.ascontiguousarray(i, np.uint32) for i in Y["inds"]]
         y = ffi.new("ptiSemiSparseTensor *")
         y.nmodes, y.mode, y.nnz, y.stride = N, mode, nf, st
         y.ndims = _ptr(keep["dims"], "ptiIndex *")
         vecs = ffi.new("ptiIndexVector[]", N)
+        keep["vecs"] = vecs
         for m in range(N):
             vecs[m].len = vecs[m].cap = keep["inds"][m].size
             vecs[m].data = _ptr(keep["inds"][m], "ptiIndex *") if keep["inds"][m].size else ffi.NULL
         y.inds = vecs
         y.values.nrows, y.values.ncols, y.values.cap, y.values.stride = nf, st, nf, st
         y.values.values = _ptr(keep["vals"], "ptiValue *") if nf else ffi.NULL
+        return y
+
+    @classmethod
+    def semi_sparse_ttm(cls, Y, U):
+        """ptiSemiSparseTensorMulMatrix on a ttm()/ttv() result: its dense
+        fibers (ndims[mode] columns used) times U, in the same layout."""
+        keep = {}
+        y = cls._semi_struct(Y, keep)
+        U = np.ascontiguousarray(U, np.float32)
+        I, R = U.shape
+        st = ((R - 1) // 8 + 1) * 8
+        buf = np.zeros((I, st), np.float32)
+        buf[:, :R] = U
+        m = ffi.new("ptiMatrix *")
+        m.nrows, m.ncols, m.cap, m.stride = I, R, I, st
+        m.values = _ptr(buf, "ptiValue *")
+        out = ffi.new("ptiSemiSparseTensor *")
+        check(lib().ptiSemiSparseTensorMulMatrix(out, y, m, Y["mode"]), "ptiSemiSparseTensorMulMatrix")
+        return cls._semi_sparse(None, out)
+
+    @classmethod
+    def from_semi_sparse(cls, Y, epsilon=1e-6) -> "COOTensor":
+        """ptiSemiSparseTensorToSparseTensor of a ttm()/ttv() result: the
+        entries that are NaN, infinite or normal with |v| >= epsilon, sorted."""
+        N = len(Y["dims"])
+        keep = {}
+        y = cls._semi_struct(Y, keep)
         t = ffi.new("ptiSparseTensor *")
         check(lib().ptiSemiSparseTensorToSparseTensor(t, y, float(epsilon)), "ptiSemiSparseTensorToSparseTensor")
         nnz = t.nnz

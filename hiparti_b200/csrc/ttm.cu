@@ -630,6 +630,66 @@ __global__ void permute_f32_t(const float *src, const uint32_t *perm, uint64_t n
     GRID_LOOP(i, n) dst[i] = src[perm[i]];
 }
 
+// Semi-sparse TTM (src/ssptensor/mmul.c:29-92): Y[i, k] = sum over r of
+// X[i, r] * U[r, k] for every fiber i, r in order, FP32 multiply-then-add.
+// One thread per (fiber, column), columns fastest so U rows are read together.
+__global__ void ssp_ttm_kernel(const float *__restrict__ X, uint32_t xs, const float *__restrict__ U, uint32_t us,
+                               uint32_t I, uint32_t R, uint64_t nfib, float *__restrict__ Y, uint32_t ys)
+{
+    GRID_LOOP(e, nfib * ys)
+    {
+        const uint64_t i = e / ys;
+        const uint32_t k = (uint32_t)(e - i * ys);
+        float acc = 0.f;
+        if (k < R) {
+            const float *x = X + i * xs;
+            for (uint32_t r = 0; r < I; ++r) acc = __fadd_rn(acc, __fmul_rn(x[r], __ldg(U + (size_t)r * us + k)));
+        }
+        Y[e] = acc;
+    }
+}
+
+int ssp_ttm(ptiSemiSparseTensor *Y, const ptiSemiSparseTensor *X, const ptiMatrix *U, uint32_t mode)
+{
+    const char *mod = "SspTns * Mtx";
+    PTI_CHECK(Y && X && U, PTIERR_VALUE_ERROR, mod, "null argument");
+    PTI_CHECK(mode < X->nmodes && X->ndims[mode] == U->nrows, PTIERR_SHAPE_MISMATCH, mod, "shape mismatch");
+    const uint32_t N = X->nmodes, I = U->nrows, R = U->ncols;
+    PTI_CHECK(I <= X->stride || X->nnz == 0, PTIERR_SHAPE_MISMATCH, mod, "fibers shorter than U's rows");
+    PTI_CHECK(U->stride >= R, PTIERR_SHAPE_MISMATCH, mod, "U's stride below its column count");
+    std::vector<ptiIndex> nd(X->ndims, X->ndims + N);
+    nd[mode] = R;
+    PTI_TRY(ptiNewSemiSparseTensor(Y, N, mode, nd.data()));
+    const uint64_t nfib = X->nnz;
+    const uint32_t ys = Y->stride;
+    for (uint32_t m = 0; m < N; ++m) {
+        if (m == mode) continue;
+        std::free(Y->inds[m].data);
+        const uint64_t len = X->inds[m].len;
+        Y->inds[m].len = Y->inds[m].cap = len;
+        Y->inds[m].data = static_cast<ptiIndex *>(std::malloc((len ? len : 1) * sizeof(ptiIndex)));
+        PTI_CHECK(Y->inds[m].data, PTIERR_OS_ERROR + ENOMEM, mod, "out of memory");
+        if (len) std::memcpy(Y->inds[m].data, X->inds[m].data, len * sizeof(ptiIndex));
+    }
+    ptiFreeMatrix(&Y->values);
+    PTI_TRY(ptiNewMatrix(&Y->values, (ptiIndex)nfib, ys));
+    Y->nnz = nfib;
+    if (!nfib) return 0;
+    cudaStream_t s = sync_stream();
+    DevBuf dx, du, dy;
+    PTI_CUDA(dx.alloc(padded(nfib * X->stride * 4), s), mod);
+    PTI_CUDA(du.alloc(padded((size_t)I * U->stride * 4), s), mod);
+    PTI_CUDA(dy.alloc(padded(nfib * ys * 4), s), mod);
+    PTI_CUDA(cudaMemcpyAsync(dx.ptr, X->values.values, nfib * X->stride * 4, cudaMemcpyHostToDevice, s), mod);
+    if (I) PTI_CUDA(cudaMemcpyAsync(du.ptr, U->values, (size_t)I * U->stride * 4, cudaMemcpyHostToDevice, s), mod);
+    ssp_ttm_kernel<<<grid_t(nfib * ys), 256, 0, s>>>(dx.as<float>(), X->stride, du.as<float>(), U->stride, I, R, nfib,
+                                                     dy.as<float>(), ys);
+    PTI_CUDA(cudaGetLastError(), mod);
+    PTI_CUDA(cudaMemcpyAsync(Y->values.values, dy.ptr, nfib * ys * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
 int ssp_to_sparse(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, float eps)
 {
     const char *mod = "SspTns -> SpTns";
@@ -714,6 +774,19 @@ int ssp_to_sparse(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, float e
 }  // namespace pti
 
 extern "C" {
+
+// include/includes/ssptensors.h:49-50, src/ssptensor/mmul.c:29-92 and
+// mmul_cuda.cu:46-: the semi-sparse TTM, both variants on the GPU.
+int ptiSemiSparseTensorMulMatrix(ptiSemiSparseTensor *Y, const ptiSemiSparseTensor *X, const ptiMatrix *U,
+                                 ptiIndex mode)
+{
+    return pti::ssp_ttm(Y, X, U, mode);
+}
+int ptiCudaSemiSparseTensorMulMatrix(ptiSemiSparseTensor *Y, const ptiSemiSparseTensor *X, const ptiMatrix *U,
+                                     ptiIndex mode)
+{
+    return pti::ssp_ttm(Y, X, U, mode);
+}
 
 // include/includes/ssptensors.h:26, src/sptensor/fromssp.c:32-84, computed on
 // the GPU.  epsilon >= 0 (the reference asserts epsilon > 0; with 0 it keeps

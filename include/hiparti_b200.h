@@ -251,6 +251,13 @@ int ptiSparseTensorMulVector(ptiSemiSparseTensor *Y, ptiSparseTensor * const X, 
  * of src that are NaN, infinite or normal with |v| >= epsilon, as a sparse
  * tensor sorted lexicographically (dest uninitialised; epsilon >= 0). */
 int ptiSemiSparseTensorToSparseTensor(ptiSparseTensor *dest, const ptiSemiSparseTensor *src, ptiValue epsilon);
+/* include/includes/ssptensors.h:49-50, src/ssptensor/mmul.c:29-92: a semi-sparse
+ * tensor's dense fibers times U (X->ndims[mode] x R): Y[i, k] = sum_r X[i, r] U[r, k]
+ * in order, FP32 multiply-then-add (bit-identical); Y uninitialised. */
+int ptiSemiSparseTensorMulMatrix(ptiSemiSparseTensor *Y, const ptiSemiSparseTensor *X, const ptiMatrix *U,
+                                 ptiIndex mode);
+int ptiCudaSemiSparseTensorMulMatrix(ptiSemiSparseTensor *Y, const ptiSemiSparseTensor *X, const ptiMatrix *U,
+                                     ptiIndex mode);
 
 /* ---------------------------------------------------------------------------
  * MTTKRP.  mats[0..N-1] are the factor matrices (row i of mats[k] is the rank-R

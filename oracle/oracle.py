@@ -351,6 +351,33 @@ class Ref:
         inds = [_np_from(t.inds[m].data, nnz, np.uint32) for m in range(N)]
         return inds, _np_from(t.values.data, nnz, np.float32)
 
+    def ssp_ttm(self, Y, U):
+        """ptiSemiSparseTensorMulMatrix of the reference on a ttm() result dict.
+        Returns (fiber inds per mode, values nfibers x stride)."""
+        N, mode = len(Y["dims"]), Y["mode"]
+        nf, st = Y["vals"].shape
+        keep = {"dims": np.asarray(Y["dims"], np.uint32).copy(),
+                "vals": np.ascontiguousarray(Y["vals"], np.float32).copy(),
+                "inds": [np.ascontiguousarray(i, np.uint32).copy() for i in Y["inds"]]}
+        vecs = (_Vec * N)(*[_Vec(keep["inds"][m].size, keep["inds"][m].size, keep["inds"][m].ctypes.data)
+                            for m in range(N)])
+        y = _SemiSparse(N, keep["dims"].ctypes.data, mode, nf, vecs, st,
+                        _Matrix(nf, st, nf, st, keep["vals"].ctypes.data))
+        R = U.shape[1]
+        ust = ((R - 1) // 8 + 1) * 8
+        buf = np.zeros((U.shape[0], ust), np.float32)
+        buf[:, :R] = U
+        m = _Matrix(U.shape[0], R, U.shape[0], ust, buf.ctypes.data)
+        out = _SemiSparse()
+        rc = self.L.ptiSemiSparseTensorMulMatrix(C.byref(out), C.byref(y), C.byref(m), C.c_uint32(mode))
+        assert rc == 0
+        n2, st2 = int(out.nnz), int(out.stride)
+        finds = [_np_from(out.inds[k].data, int(out.inds[k].len), np.uint32) if out.inds[k].len
+                 else np.empty(0, np.uint32) for k in range(N)]
+        vals = _np_from(out.values.values, n2 * st2, np.float32).reshape(n2, st2) if n2 else \
+            np.empty((0, st2), np.float32)
+        return finds, vals
+
     def orderit(self, dims, inds, vals, iterations):
         """orderit(renumber=1) of the reference (src/sptensor/orderit.c:121-208),
         its Lexi-order driver with a correct coordinate sort."""

@@ -133,3 +133,21 @@ def test_semi_sparse_to_sparse_matches_reference(lib, cuda, ref, eps):
     for a, b in zip(got.inds, want_inds):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(got.vals.view(np.uint32), want_vals.view(np.uint32))
+
+
+@pytest.mark.parametrize("R2", [3, 8, 20])
+def test_semi_sparse_ttm_matches_reference(lib, cuda, ref, R2):
+    """ptiSemiSparseTensorMulMatrix (src/ssptensor/mmul.c): a TTM result's
+    dense fibers times a second matrix, bit for bit against the reference."""
+    dims = (40, 30, 25)
+    inds, vals = _tensor(dims, 4000, 21)
+    U = np.random.default_rng(22).standard_normal((25, 12)).astype(np.float32)
+    coo = COOTensor(dims, [i.copy() for i in inds], vals.copy())
+    Y = coo.ttm(U, 2)
+    V = np.random.default_rng(23).standard_normal((12, R2)).astype(np.float32)
+    want_inds, want_vals = ref.ssp_ttm(Y, V)
+    got = COOTensor.semi_sparse_ttm(Y, V)
+    assert got["dims"][2] == R2
+    for a, b in zip(got["inds"], want_inds):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(got["vals"].view(np.uint32), want_vals.view(np.uint32))
