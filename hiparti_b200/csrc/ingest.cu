@@ -42,6 +42,11 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <fcntl.h>
+#include <mutex>
+#include <sys/stat.h>
+#include <thread>
+#include <unistd.h>
 
 #include "primitives.cuh"
 #include "tensor.cuh"
@@ -58,7 +63,7 @@ constexpr int kIngStep = kIngThreads * kIngSeg;                 // 4 KB
 constexpr int kIngChunk = kIngStep * kIngSteps;                 // 16 KB per CTA
 constexpr uint32_t kMaxToken = 4096;
 constexpr int kMaxSigDigits = 100;
-constexpr size_t kReadChunk = 32ull << 20;                      // pinned read buffer
+constexpr size_t kReadChunk = 16ull << 20;                      // pinned read buffer
 
 // Error flags of the parse (bit set in ParseSlots::fatal_flags)
 constexpr uint32_t kFatalHex = 1, kFatalNanPayload = 2, kFatalLong = 4, kFatalDigits = 8;
@@ -562,57 +567,115 @@ int dedupe_coo(ptiB200Tensor *t, cudaStream_t s)
 
 namespace {
 
+// Pinned staging for file reads, kept for the life of the process: kReaders
+// reader threads with two kReadChunk buffers each, every thread with its own
+// stream and an event per buffer.  Loads are serialised on its mutex.
+constexpr int kReaders = 4;
+struct ReadPool {
+    std::mutex mu;
+    bool ready = false;
+    unsigned char *pin[kReaders][2] = {};
+    cudaStream_t st[kReaders] = {};
+    cudaEvent_t ev[kReaders][2] = {};
+};
+ReadPool &read_pool(int dev)
+{
+    static ReadPool p[64];  // per device: the streams and events belong to one
+    return p[dev & 63];
+}
+
 // Reads the whole file into a device buffer padded with spaces to
-// `pad_to`-byte multiples (+64), through two pinned buffers.
+// `pad_to`-byte multiples (+64).  kReaders threads pread interleaved chunks
+// of kReadChunk bytes into pinned buffers (two per thread) and copy each to
+// its place on the device on their own streams, so reading the page cache,
+// which one thread cannot do at link speed, runs in parallel and overlaps
+// the copies.
 int read_to_device(const char *fname, DevBuf &dbuf, uint64_t &len, std::vector<unsigned char> &head,
                    size_t head_bytes, uint64_t pad_to, cudaStream_t s)
 {
     const char *mod = "B200 SpTns Load";
-    FILE *fp = std::fopen(fname, "rb");
-    PTI_CHECK(fp, PTIERR_OS_ERROR + errno, mod, std::strerror(errno));
-    std::fseek(fp, 0, SEEK_END);
-    const long flen = std::ftell(fp);
-    std::fseek(fp, 0, SEEK_SET);
-    if (flen < 0) {
-        std::fclose(fp);
-        PTI_FAIL(PTIERR_OS_ERROR + EIO, mod, "cannot size the file");
+    const int fd = open(fname, O_RDONLY);
+    PTI_CHECK(fd >= 0, PTIERR_OS_ERROR + errno, mod, std::strerror(errno));
+    struct stat stbuf;
+    if (fstat(fd, &stbuf) != 0) {
+        const int e = errno;
+        close(fd);
+        PTI_FAIL(PTIERR_OS_ERROR + e, mod, "cannot size the file");
     }
-    len = (uint64_t)flen;
+    len = (uint64_t)stbuf.st_size;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    ReadPool &P = read_pool(dev);
+    std::lock_guard<std::mutex> lock(P.mu);
+    cudaError_t ce = cudaSuccess;
+    if (!P.ready) {
+        for (int t = 0; t < kReaders && ce == cudaSuccess; ++t) {
+            ce = cudaStreamCreateWithFlags(&P.st[t], cudaStreamNonBlocking);
+            for (int b = 0; b < 2 && ce == cudaSuccess; ++b) {
+                ce = cudaHostAlloc(reinterpret_cast<void **>(&P.pin[t][b]), kReadChunk, cudaHostAllocDefault);
+                if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&P.ev[t][b], cudaEventDisableTiming);
+            }
+        }
+        if (ce != cudaSuccess) {
+            close(fd);
+            PTI_CUDA(ce, mod);
+        }
+        P.ready = true;
+    }
     const uint64_t alloc = std::max<uint64_t>(1, (len + pad_to - 1) / pad_to) * pad_to + 64;
-    int rc = 0;
-    cudaError_t ce = dbuf.alloc(alloc, s);
+    cudaEvent_t filled = nullptr;
+    ce = dbuf.alloc(alloc, s);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(dbuf.ptr, ' ', alloc, s);
-    unsigned char *pin[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    for (int b = 0; b < 2 && ce == cudaSuccess; ++b) {
-        ce = cudaHostAlloc(reinterpret_cast<void **>(&pin[b]), kReadChunk, cudaHostAllocDefault);
-        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&filled, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventRecord(filled, s);
+    if (ce != cudaSuccess) {
+        close(fd);
+        if (filled) cudaEventDestroy(filled);
+        PTI_CUDA(ce, mod);
     }
     head.assign(std::min<uint64_t>(head_bytes, len), 0);
-    uint64_t done = 0;
-    for (int b = 0; ce == cudaSuccess && done < len; b ^= 1) {
-        ce = cudaEventSynchronize(ev[b]);  // the buffer's previous copy has landed
-        if (ce != cudaSuccess) break;
-        const size_t want = (size_t)std::min<uint64_t>(kReadChunk, len - done);
-        const size_t got = std::fread(pin[b], 1, want, fp);
-        if (got != want) {
-            rc = complain(mod, PTIERR_OS_ERROR + EIO, __FILE__, __LINE__, "short read");
-            break;
+    const uint64_t nchunks = (len + kReadChunk - 1) / kReadChunk;
+    const int nthreads = (int)std::min<uint64_t>(kReaders, std::max<uint64_t>(nchunks, 1));
+    std::vector<int> err(nthreads, 0);
+    std::vector<cudaError_t> cerr(nthreads, cudaSuccess);
+    auto reader = [&](int t) {
+        cudaError_t c = cudaSetDevice(dev);
+        if (c == cudaSuccess) c = cudaStreamWaitEvent(P.st[t], filled, 0);  // after the fill with spaces
+        int slot = 0;
+        for (uint64_t k = t; c == cudaSuccess && k < nchunks; k += nthreads, slot ^= 1) {
+            c = cudaEventSynchronize(P.ev[t][slot]);  // the buffer's previous copy has landed
+            if (c != cudaSuccess) break;
+            const uint64_t off = k * kReadChunk;
+            const size_t want = (size_t)std::min<uint64_t>(kReadChunk, len - off);
+            size_t got = 0;
+            while (got < want) {
+                const ssize_t r = pread(fd, P.pin[t][slot] + got, want - got, (off_t)(off + got));
+                if (r <= 0) break;
+                got += (size_t)r;
+            }
+            if (got != want) {
+                err[t] = EIO;
+                break;
+            }
+            if (off < head.size())
+                std::memcpy(head.data() + off, P.pin[t][slot], std::min<uint64_t>(want, head.size() - off));
+            c = cudaMemcpyAsync(dbuf.as<unsigned char>() + off, P.pin[t][slot], want, cudaMemcpyHostToDevice,
+                                P.st[t]);
+            if (c == cudaSuccess) c = cudaEventRecord(P.ev[t][slot], P.st[t]);
         }
-        if (done < head.size()) std::memcpy(head.data() + done, pin[b], std::min<uint64_t>(got, head.size() - done));
-        ce = cudaMemcpyAsync(dbuf.as<unsigned char>() + done, pin[b], got, cudaMemcpyHostToDevice, s);
-        if (ce == cudaSuccess) ce = cudaEventRecord(ev[b], s);
-        done += got;
+        if (c == cudaSuccess) c = cudaStreamSynchronize(P.st[t]);
+        cerr[t] = c;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(reader, t);
+    reader(0);
+    for (auto &th : pool) th.join();
+    close(fd);
+    cudaEventDestroy(filled);
+    for (int t = 0; t < nthreads; ++t) {
+        PTI_CHECK(!err[t], PTIERR_OS_ERROR + err[t], mod, "short read");
+        PTI_CUDA(cerr[t], mod);
     }
-    std::fclose(fp);
-    cudaError_t ce2 = cudaStreamSynchronize(s);
-    for (int b = 0; b < 2; ++b) {
-        if (ev[b]) cudaEventDestroy(ev[b]);
-        if (pin[b]) cudaFreeHost(pin[b]);
-    }
-    if (rc) return rc;
-    PTI_CUDA(ce, mod);
-    PTI_CUDA(ce2, mod);
     return 0;
 }
 

@@ -383,7 +383,9 @@ int ptiB200TensorInfo(ptiB200Tensor const *t, ptiNnzIndex info[7], ptiIndex *ndi
  * first) and replaces each repeated coordinate by one nonzero holding the FP32
  * sum of its values in file order.  Indices must fit the mode sizes.  Hex
  * values, nan(...) payloads, values with more than 100 significant digits and
- * tokens longer than 4096 bytes are rejected.  Synchronous on `stream`. */
+ * tokens longer than 4096 bytes are rejected.  The first load on a device
+ * keeps 128 MB of pinned host staging (4 reader threads x 2 x 16 MB) for later
+ * loads.  Synchronous on `stream`. */
 int ptiB200LoadSparseTensor(ptiB200Tensor **out, ptiIndex start_index, const char *fname, int dedupe,
                             void *stream);
 /* Copies a device COO tensor's arrays to host buffers: inds[m] and vals, nnz
