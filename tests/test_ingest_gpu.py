@@ -158,7 +158,8 @@ def _write_bin(path, dims, inds, vals, vw):
                 struct.pack("<I", vals.size))
         for i in inds:
             f.write(np.asarray(i, np.uint32).tobytes())
-        f.write(np.asarray(vals, np.float32 if vw == 4 else np.float64).tobytes())
+        with np.errstate(over="ignore"):  # values beyond FP32 become infinities on purpose
+            f.write(np.asarray(vals, np.float32 if vw == 4 else np.float64).tobytes())
 
 
 @pytest.mark.parametrize("vw", [4, 8])
