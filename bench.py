@@ -399,6 +399,43 @@ def run_ttm(args):
     return out
 
 
+def run_c2_sk20(args):
+    """The C2 tensor converted with sk = 20 (one HiCOO kernel, the setting of
+    the reference's single-kernel sweeps) instead of sk = 10: conversion time
+    and the all-mode MTTKRP time.  The MTTKRP schedule is built from blocks,
+    so sk should change the conversion's kernel pointers and schedule only."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    coo, h, inds, vals, conv10 = make_c2(dev, SEED)
+    facs = c2_factors(dev, SEED)
+    out = {"workload": "C2 HiCOO MTTKRP with sk=20 (single kernel) against sk=10, sb=7, R=32 FP32"}
+    for sk, t in ((10, h), (20, None)):
+        if t is None:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            t = coo.to_hicoo(C2_SB, 20, C2_SC)
+            torch.cuda.synchronize()
+            conv = time.perf_counter() - t0
+        else:
+            conv = conv10
+        t.prepare()
+        for m in range(3):
+            t.mttkrp(facs, m, rank=C2_R)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            for m in range(3):
+                t.mttkrp(facs, m, rank=C2_R)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"sk{sk}"] = {"conversion_s": round(conv, 4), "mttkrp_ms_all_modes": round(e0.elapsed_time(e1) / 5, 3),
+                          "nb": t.nb}
+        t.free()
+    coo.free()
+    return out
+
+
 RENUM_REF_NNZ = 200_000
 
 
@@ -1036,7 +1073,8 @@ def main():
     ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
     ap.add_argument("--no-renumber", action="store_true", help="skip the renumbering block")
     ap.add_argument("--no-ttm", action="store_true", help="skip the TTM block")
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm", "cpu_paths"],
+    ap.add_argument("--no-sk20", action="store_true", help="skip the C2 sk=20 block")
+    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm", "cpu_paths", "sk20"],
                     default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
@@ -1065,7 +1103,8 @@ def main():
         import torch
         torch.cuda.set_device(0)
         block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
-                 "renumber": run_renumber, "ttm": run_ttm, "cpu_paths": run_cpu_paths}[args.only]
+                 "renumber": run_renumber, "ttm": run_ttm, "cpu_paths": run_cpu_paths,
+                 "sk20": run_c2_sk20}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
         return
     rank, world, _ = dist_setup(args.gpus)
@@ -1098,6 +1137,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["ttm"] = run_ttm(args)
+        if world == 1 and not args.no_sk20:
+            import torch
+            torch.cuda.empty_cache()
+            res["c2_sk20"] = run_c2_sk20(args)
         print(json.dumps(res), flush=True)
     from hiparti_b200 import replicas
     replicas.shutdown(world)

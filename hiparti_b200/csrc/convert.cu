@@ -168,7 +168,14 @@ struct KernelOut {
 };
 
 // Greedy chunk pointers of one kernel (convert.c:737-742, 805-815); writes
-// them if `out` is non-null, otherwise stores their count.
+// them if `out` is non-null, otherwise stores their count.  The reference
+// walks the kernel's blocks keeping a running nonzero count that resets
+// after each emitted chunk: at block step s (the count of block s-1 added)
+// a chunk is emitted when the count reaches 2^sc.  A step's count is
+// bptr[s] - bptr[s0 - 1], s0 the first step after the last reset, and bptr
+// increases strictly, so the next emission is the first s >= s0 with
+// bptr[s] >= bptr[s0 - 1] + 2^sc: a binary search per chunk instead of a
+// step per block (one kernel can hold all blocks when sk is large).
 __device__ uint64_t kernel_chunks(uint64_t k, const uint64_t *kptr, const uint64_t *bptr, uint64_t sc,
                                   uint64_t *out)
 {
@@ -176,26 +183,20 @@ __device__ uint64_t kernel_chunks(uint64_t k, const uint64_t *kptr, const uint64
     uint64_t n = 0;
     if (out) out[n] = first;
     ++n;
-    uint32_t chunk = 0;
-    if (k > 0) {  // the kernel's first block closes the previous kernel's last block
-        uint64_t ne = bptr[first] - bptr[first - 1];
-        if ((uint64_t)chunk + ne >= sc) {
-            if (out) out[n] = first;
-            ++n;
-            chunk = 0;
-        } else {
-            chunk += (uint32_t)ne;
+    // the first step of kernel k > 0 adds the previous kernel's last block
+    uint64_t s0 = k > 0 ? first : first + 1;
+    while (s0 < last) {
+        const uint64_t target = bptr[s0 - 1] + sc;
+        uint64_t lo = s0, hi = last;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (bptr[mid] >= target) hi = mid;
+            else lo = mid + 1;
         }
-    }
-    for (uint64_t j = first + 1; j < last; ++j) {
-        uint64_t ne = bptr[j] - bptr[j - 1];
-        if ((uint64_t)chunk + ne >= sc) {
-            if (out) out[n] = j;
-            ++n;
-            chunk = 0;
-        } else {
-            chunk += (uint32_t)ne;
-        }
+        if (lo == last) break;
+        if (out) out[n] = lo;
+        ++n;
+        s0 = lo + 1;
     }
     return n;
 }
