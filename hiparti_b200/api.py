@@ -447,6 +447,13 @@ class DeviceTensor:
         for m in modes:
             check(lib().ptiB200Prepare(self._h, m, stream), "ptiB200Prepare")
 
+    def check(self):
+        """Waits for the current stream and raises if this tensor's kernels
+        recorded a device error (ptiB200CheckTensor)."""
+        import torch
+        stream = ffi.cast("void *", torch.cuda.current_stream().cuda_stream)
+        check(lib().ptiB200CheckTensor(self._h, stream), "ptiB200CheckTensor")
+
     def mttkrp(self, factors, mode, rank=None, out=None, mats_order=None):
         """factors: list of CUDA tensors (I_k, stride), float32 or bfloat16, all
         of one dtype; returns / fills a float32 (I_mode, stride) tensor."""

@@ -502,7 +502,6 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
 }
 
 int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
-int take_device_error(cudaStream_t s, const char *mod);
 
 namespace {
 

@@ -52,7 +52,6 @@
 #include "tensor.cuh"
 
 namespace pti {
-int take_device_error(cudaStream_t s, const char *mod);
 
 namespace {
 

@@ -217,8 +217,8 @@ void launch_hicoo(const HicooArgs &a, int G, unsigned ntiles, cudaStream_t s)
 
 }  // namespace
 
-int ensure_err_word(cudaStream_t s);
-uint32_t *err_word();
+int ensure_err_word(ptiB200Tensor *t, cudaStream_t s);
+uint32_t *err_word(ptiB200Tensor *t);
 int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                      const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
                      const float *vals_override);
@@ -292,7 +292,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
         return 0;
     }
 
-    PTI_TRY(ensure_err_word(s));
+    PTI_TRY(ensure_err_word(t, s));
     HicooArgs a{};
     a.nnz = t->nnz;
     a.nb = t->nb;
@@ -314,7 +314,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     }
     a.vals = t->vals.as<float>();
     a.out = out;
-    a.err = err_word();
+    a.err = err_word(t);
     if (ft == PTI_B200_F32) launch_hicoo<float>(a, G, t->ntiles, s);
     else launch_hicoo<__nv_bfloat16>(a, G, t->ntiles, s);
     PTI_CUDA(cudaGetLastError(), mod);
@@ -322,40 +322,32 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
 }
 
 // ----------------------------------------------------------------------------
-// Device error word: set by kernels that meet an out-of-range coordinate.
+// Device error word of a tensor: set by kernels that meet an out-of-range
+// coordinate or give up a bounded wait.  One word per tensor handle, so calls
+// on different tensors (different streams or host threads) do not see each
+// other's errors.
 // ----------------------------------------------------------------------------
-namespace {
-std::vector<uint32_t *> g_err;
-}
-
-int ensure_err_word(cudaStream_t s)
+int ensure_err_word(ptiB200Tensor *t, cudaStream_t s)
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if ((int)g_err.size() <= dev) g_err.resize(dev + 1, nullptr);
-    if (!g_err[dev]) {
-        PTI_CUDA(cudaMalloc(&g_err[dev], sizeof(uint32_t)), "B200 err");
-        PTI_CUDA(cudaMemsetAsync(g_err[dev], 0, sizeof(uint32_t), s), "B200 err");
+    if (!t->err.ptr) {
+        PTI_CUDA(t->err.alloc(padded(sizeof(uint32_t)), s), "B200 err");
+        PTI_CUDA(cudaMemsetAsync(t->err.ptr, 0, sizeof(uint32_t), s), "B200 err");
     }
     return 0;
 }
 
-uint32_t *err_word()
-{
-    int dev = 0;
-    cudaGetDevice(&dev);
-    return dev < (int)g_err.size() ? g_err[dev] : nullptr;
-}
+uint32_t *err_word(ptiB200Tensor *t) { return t->err.as<uint32_t>(); }
 
-// Reads and clears the device error word (synchronises `s`).
-int take_device_error(cudaStream_t s, const char *mod)
+// Reads and clears the tensor's device error word (synchronises `s`).
+int take_device_error(ptiB200Tensor *t, cudaStream_t s, const char *mod)
 {
-    uint32_t *w = err_word();
+    uint32_t *w = err_word(t);
     if (!w) return 0;
     uint32_t h = 0;
     PTI_CUDA(cudaMemcpyAsync(&h, w, sizeof h, cudaMemcpyDeviceToHost, s), mod);
     PTI_CUDA(cudaMemsetAsync(w, 0, sizeof h, s), mod);
     PTI_CUDA(cudaStreamSynchronize(s), mod);
+    PTI_CHECK(!(h & 2u), PTIERR_CUDA_ERROR, mod, "a bulk copy did not complete within its wait limit");
     PTI_CHECK(h == 0, PTIERR_VALUE_ERROR, mod, "tensor coordinate out of range");
     return 0;
 }
@@ -388,13 +380,13 @@ int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s)
 int check_coo_ranges(ptiB200Tensor *t, cudaStream_t s)
 {
     const char *mod = "B200 Upload";
-    PTI_TRY(ensure_err_word(s));
+    PTI_TRY(ensure_err_word(t, s));
     if (t->nnz) {
         for (uint32_t m = 0; m < t->nmodes; ++m)
             check_coo_kernel<<<grid_for(t->nnz, 256), 256, 0, s>>>(t->inds[m].as<uint32_t>(), t->nnz,
-                                                                   t->ndims[m], err_word());
+                                                                   t->ndims[m], err_word(t));
         PTI_CUDA(cudaGetLastError(), mod);
-        PTI_TRY(take_device_error(s, mod));
+        PTI_TRY(take_device_error(t, s, mod));
     }
     return 0;
 }
@@ -403,13 +395,13 @@ int check_coo_ranges(ptiB200Tensor *t, cudaStream_t s)
 int validate_coo(ptiB200Tensor *t, cudaStream_t s)
 {
     const char *mod = "B200 Upload";
-    PTI_TRY(ensure_err_word(s));
+    PTI_TRY(ensure_err_word(t, s));
     if (t->nnz) {
         for (uint32_t m = 0; m < t->nmodes; ++m)
             check_coo_kernel<<<grid_for(t->nnz, 256), 256, 0, s>>>(t->inds[m].as<uint32_t>(), t->nnz,
-                                                                   t->ndims[m], err_word());
+                                                                   t->ndims[m], err_word(t));
         PTI_CUDA(cudaGetLastError(), mod);
-        PTI_TRY(take_device_error(s, mod));
+        PTI_TRY(take_device_error(t, s, mod));
     }
     return 0;
 }
@@ -474,12 +466,12 @@ int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s
     if (t->nnz)
         PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s2 ? s2 : s), mod);
     if (s2 && late) PTI_CUDA(cudaEventRecord(late, s2), mod);
-    PTI_TRY(ensure_err_word(s));
+    PTI_TRY(ensure_err_word(t, s));
     if (t->nb) {
         check_bptr_kernel<<<grid_for(t->nb + 1, 256), 256, 0, s>>>(t->bptr.as<uint64_t>(), t->nb, t->nnz,
-                                                                   err_word());
+                                                                   err_word(t));
         PTI_CUDA(cudaGetLastError(), mod);
-        PTI_TRY(take_device_error(s, mod));
+        PTI_TRY(take_device_error(t, s, mod));
     }
     return finish_hicoo_layout(t, s);
 }
@@ -524,7 +516,7 @@ int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, pti
     PTI_CUDA(dout.alloc(padded(obytes), s), mod);
     PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s, nullptr, late));
     PTI_CUDA(cudaMemcpyAsync(mats[N]->values, dout.ptr, obytes, cudaMemcpyDeviceToHost, s), mod);
-    PTI_TRY(take_device_error(s, mod));
+    PTI_TRY(take_device_error(t, s, mod));
     return 0;
 }
 
@@ -785,6 +777,12 @@ int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream)
 {
     PTI_CHECK(t, PTIERR_VALUE_ERROR, "B200 Prepare", "null handle");
     return pti::prepare_mode(t, mode, static_cast<cudaStream_t>(stream));
+}
+
+int ptiB200CheckTensor(ptiB200Tensor *t, void *stream)
+{
+    PTI_CHECK(t, PTIERR_VALUE_ERROR, "B200 Check", "null handle");
+    return pti::take_device_error(t, static_cast<cudaStream_t>(stream), "B200 Check");
 }
 
 }  // extern "C"

@@ -32,8 +32,8 @@ constexpr int kTile = 2048;        // nonzeros per CTA (COO kernel)
 constexpr int kHiTile = kPlanTile; // nonzeros per CTA (HiCOO kernel)
 constexpr int kSchedThreads = 256;
 
-uint32_t *err_word();
-int ensure_err_word(cudaStream_t s);
+uint32_t *err_word(ptiB200Tensor *t);
+int ensure_err_word(ptiB200Tensor *t, cudaStream_t s);
 
 struct SchedArgs {
     uint64_t nnz, nb;
@@ -841,14 +841,14 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
 {
     const char *mod = "B200 MTTKRP";
     const uint32_t N = t->nmodes;
-    PTI_TRY(ensure_err_word(s));
+    PTI_TRY(ensure_err_word(t, s));
     SchedArgs a{};
     a.nnz = t->nnz;
     a.R = R;
     a.stride = stride;
     a.out_dim = t->ndims[mode];
     a.out = out;
-    a.err = err_word();
+    a.err = err_word(t);
     const uint32_t *recs = nullptr;
     unsigned ntiles;
     if (t->hicoo) {

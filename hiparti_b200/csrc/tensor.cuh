@@ -77,6 +77,8 @@ struct ptiB200Tensor {
     pti::DevBuf tile_block;                          // first block of each nnz tile
     uint32_t ntiles = 0;
 
+    pti::DevBuf err;  // uint32: device error word of this tensor's kernels
+
     std::array<pti::CooModePlan, pti::kMaxModes> coo_plan;
     std::array<pti::HicooModePlan, pti::kMaxModes> hicoo_plan;
     std::array<pti::FiberPlan, pti::kMaxModes> fiber_plan;

@@ -366,6 +366,11 @@ int ptiB200ConvertToHiCOO(ptiB200Tensor **out, ptiB200Tensor *coo, ptiElementInd
                           ptiNnzIndex *nb, ptiNnzIndex *max_nnzb, void *stream);
 /* Build the per-mode schedule for `mode` now (otherwise built on first use). */
 int ptiB200Prepare(ptiB200Tensor *t, ptiIndex mode, void *stream);
+/* Waits for `stream` and reports (then clears) an error that the tensor's
+ * asynchronous kernels recorded on the device: PTIERR_VALUE_ERROR for a
+ * coordinate outside its mode, PTIERR_CUDA_ERROR for a tile copy that did not
+ * complete within its wait limit; 0 when there was none. */
+int ptiB200CheckTensor(ptiB200Tensor *t, void *stream);
 int ptiB200FreeTensor(ptiB200Tensor *t);
 /* Copies a device HiCOO tensor's arrays to host buffers: bptr (nb+1),
  * binds[m] (nb each), einds[m] (nnz each), vals (nnz).  Synchronous. */

@@ -167,6 +167,7 @@ def test_device_api_torch(lib, cuda, orc, fmt, dtype):
         torch.cuda.synchronize()
         ref = orc.mttkrp_coo(inds, vals, ref_mats, R, m)[: dims[m]]
         assert rel_err(out.cpu().numpy(), ref) < TOL
+    dt.check()  # no device error recorded by the asynchronous calls
     dt.free()
 
 
