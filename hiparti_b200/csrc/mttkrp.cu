@@ -222,18 +222,19 @@ uint32_t *err_word(ptiB200Tensor *t);
 int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                      const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
                      const float *vals_override);
-bool schedule_supported(const ptiB200Tensor *t, uint32_t R);
+bool schedule_supported(const ptiB200Tensor *t, uint32_t R, uint32_t stride);
 
-// The output-privatised kernels (sched.cu) cover orders 2-4 and R <= 128;
-// HIPARTI_B200_SCHEDULE=0 selects the direct-atomic kernels instead.
-static bool use_schedule(const ptiB200Tensor *t, uint32_t R)
+// The output-privatised kernels (sched.cu) cover orders 2-4, R <= 128 and
+// (HiCOO) factors of fewer than 2^32 elements; HIPARTI_B200_SCHEDULE=0 selects
+// the direct-atomic kernels instead.
+static bool use_schedule(const ptiB200Tensor *t, uint32_t R, uint32_t stride)
 {
     static int env = -1;
     if (env < 0) {
         const char *e = std::getenv("HIPARTI_B200_SCHEDULE");
         env = (e && e[0] == '0') ? 0 : 1;
     }
-    return env == 1 && schedule_supported(t, R);
+    return env == 1 && schedule_supported(t, R, stride);
 }
 
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
@@ -266,7 +267,7 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     PTI_CUDA(cudaMemsetAsync(out, 0, (size_t)t->ndims[mode] * stride * sizeof(float), s), mod);
     if (t->nnz == 0) return 0;
     const int G = group_lanes(R);
-    if (use_schedule(t, R)) {
+    if (use_schedule(t, R, stride)) {
         PTI_TRY(prepare_mode(t, mode, s, late));
         if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
         return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s, vals_override);

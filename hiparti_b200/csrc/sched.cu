@@ -383,6 +383,9 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
                     ok_z = ok_z && r[k] < a.in_dim[k];
                 }
                 vv[p] = s_val[z];
+                // operand rows become element offsets (below 2^32: schedule_supported)
+#pragma unroll
+                for (int k = 0; k < NIN; ++k) r[k] *= a.stride;
                 if (NIN == 1) r[1] = __float_as_uint(vv[p]);
                 if (NIN == 2) r[2] = __float_as_uint(vv[p]);
                 rec[p] = make_uint4(ok_z ? o : kNoRow, r[0], r[1], r[2]);
@@ -426,6 +429,9 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         s_slot_whole[g] = 0;
     }
     RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
+    const FT *base[NIN];  // this lane's columns of each operand factor
+#pragma unroll
+    for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + col;
     for (uint32_t j = j0; j < j1; j += U) {
         uint32_t orow[U];
         float v[U];
@@ -440,8 +446,7 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
                 v[u] = NIN == 3 ? s_v3[j + u] : __uint_as_float(NIN == 2 ? r.w : r.z);
                 if (orow[u] != kNoRow && active) {
 #pragma unroll
-                    for (int k = 0; k < NIN; ++k)
-                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)rr[k] * a.stride, col);
+                    for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + rr[k], 0);
                 }
             }
         }
@@ -828,9 +833,14 @@ static int launch_n(int nin, bool hicoo, bool wide, const SchedArgs &a, const ui
     }
 }
 
-bool schedule_supported(const ptiB200Tensor *t, uint32_t R)
+bool schedule_supported(const ptiB200Tensor *t, uint32_t R, uint32_t stride)
 {
-    return t->nmodes >= 2 && t->nmodes <= 4 && R >= 1 && R <= 128;
+    if (!(t->nmodes >= 2 && t->nmodes <= 4 && R >= 1 && R <= 128)) return false;
+    // the HiCOO kernel addresses factor rows by 32-bit element offsets
+    if (t->hicoo)
+        for (uint32_t m = 0; m < t->nmodes; ++m)
+            if ((uint64_t)t->ndims[m] * stride >= ((uint64_t)1 << 32)) return false;
+    return true;
 }
 
 // Runs the scheduled kernel for `mode` (the schedule must be ready).  Output
