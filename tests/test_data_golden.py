@@ -87,3 +87,41 @@ def test_gpu_conversion_and_mttkrp_match_reference_on_examples(lib, cuda, case):
     for m in range(3):
         for variant in ["seq", "cuda"]:
             assert rel_err(hr.mttkrp(mats, R, m, variant)[: dims[m]], g[f"hicoo_out{m}"]) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", MTTKRP_FILES)
+def test_gpu_ttm_matches_reference_on_examples(lib, cuda, ref, case):
+    """ptiSparseTensorMulMatrix of the compiled reference on its example
+    tensors, every mode: fibers, coordinates and FP32 values bit for bit."""
+    g = load_golden(case)
+    dims, inds, vals = _tensor(g)
+    rng = np.random.default_rng(len(case))
+    for mode in range(3):
+        U = rng.standard_normal((dims[mode], 8)).astype(np.float32)
+        finds, yv, (xinds, xvals, xso) = ref.ttm(dims, inds, vals, U, mode)
+        coo = COOTensor(dims, [i.copy() for i in inds], vals.copy())
+        ours = coo.ttm(U, mode)
+        for a, b in zip(ours["inds"], finds):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(ours["vals"].view(np.uint32), yv.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt", ["coo", "hicoo"])
+def test_gpu_cpd_on_example_tensor(lib, cuda, orc, fmt):
+    """CPD-ALS of the 12031-nonzero example tensor (integer values 1..14),
+    R = 8, 10 iterations from seeded factors: every fit within 1e-4 of the
+    FP64 oracle's, and the final fit equal to the model's fit evaluated at
+    the nonzeros."""
+    from test_cpd_gpu import _device_cpd
+    g = load_golden("data_3D_12031.npz")
+    dims, inds, vals = _tensor(g)
+    R, iters = 8, 10
+    rng = np.random.default_rng(12031)
+    init = [np.abs(rng.standard_normal((d, R))).astype(np.float32) for d in dims]
+    lam, facs, fits = _device_cpd(dims, inds, vals, init, iters, fmt=fmt)
+    o = orc.cpd_als(dims, inds, vals, R, iters, init)
+    np.testing.assert_allclose(fits, o["fits"], atol=1e-4)
+    direct = orc.kruskal_fit(dims, inds, vals, lam.astype(np.float64), [f.astype(np.float64) for f in facs])
+    assert abs(direct - fits[-1]) < 1e-4
