@@ -53,6 +53,9 @@ cudaStream_t sync_stream();
 // A second stream per device, for host-to-device copies that overlap work on
 // sync_stream().
 cudaStream_t copy_stream();
+// Two non-blocking side streams per device (0 is copy_stream()), for kernels
+// that run beside the caller's stream; created on first use.
+cudaStream_t side_stream(int which);
 
 // Stream-ordered device allocation from the runtime's default memory pool
 // (cudaMallocAsync).  The pool keeps freed memory for reuse, so repeated calls

@@ -42,16 +42,19 @@ cudaStream_t sync_stream()
     return streams[dev];
 }
 
-cudaStream_t copy_stream()
+cudaStream_t copy_stream() { return side_stream(0); }
+
+cudaStream_t side_stream(int which)
 {
     static std::mutex mu;
-    static std::vector<cudaStream_t> streams;
+    static std::vector<cudaStream_t> streams;  // [device][2]
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
-    if ((int)streams.size() <= dev) streams.resize(dev + 1, nullptr);
-    if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
-    return streams[dev];
+    if ((int)streams.size() <= 2 * dev + 1) streams.resize(2 * dev + 2, nullptr);
+    cudaStream_t &st = streams[2 * dev + (which & 1)];
+    if (!st) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    return st;
 }
 
 void configure_pool_once()

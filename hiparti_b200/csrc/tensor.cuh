@@ -51,8 +51,11 @@ struct FiberPlan {
     DevBuf sind;                           // uint32 [nnz]: the mode's index, fiber order
     DevBuf sval;                           // float  [nnz]: values, fiber order
     DevBuf perm;                           // uint32 [nnz]: fiber-order position -> input nonzero
-    uint64_t nlong = 0;                    // fibers longer than the one-thread-per-fiber limit
-    DevBuf long_fibers;                    // uint32 [nlong]: their indices
+    uint64_t nlong = 0;                    // fibers longer than one thread takes, up to the CTA limit
+    uint64_t nvlong = 0;                   // fibers longer than that, one CTA each
+    uint64_t nshort = 0;                   // fibers one thread takes
+    DevBuf short_order;                    // uint32 [nfib]: those nshort fibers first, by length class
+    DevBuf long_fibers;                    // uint32 [nfib]: the nlong fibers from the front, the nvlong from the back
 };
 
 }  // namespace pti

@@ -23,13 +23,21 @@
 //     chains in flight at once;
 //   - ttm_kernel: a group of G lanes (G = 8, 16 or 32 by R) per fiber, each
 //     lane CPL columns; the group loads G nonzeros at a time and walks them in
-//     order.  It takes the long fibers (and every fiber when R > 32).
+//     order.  It takes every fiber when R > 32;
+//   - ttm_long_kernel and ttm_vlong_kernel (R <= 32): a warp, or for the
+//     longest fibers a CTA whose warps compute the products while one warp
+//     adds them, per fiber longer than kShortFiber.
 #include <cerrno>
 
 #include "primitives.cuh"
 #include "tensor.cuh"
+#include "tma.cuh"
 
 namespace pti {
+int ensure_err_word(ptiB200Tensor *t, cudaStream_t s);
+uint32_t *err_word(ptiB200Tensor *t);
+int take_device_error(ptiB200Tensor *t, cudaStream_t s, const char *mod);
+
 namespace {
 
 unsigned grid_t(uint64_t n)
@@ -89,27 +97,49 @@ struct FiberOut {
 
 __global__ void set_last_t(uint64_t *fptr, uint64_t nfib, uint64_t nnz) { fptr[nfib] = nnz; }
 
-constexpr uint32_t kShortFiber = 64;  // longest fiber a single thread takes
+constexpr uint32_t kShortFiber = 64;      // longest fiber a single thread takes
+constexpr uint64_t kVLongFiber = 8192;    // longer fibers get a CTA each (ttm_vlong_kernel)
 
+// Fibers longer than kShortFiber: up to kVLongFiber nonzeros from the front of
+// `list` (count[0] of them), longer ones from the back (count[1]).
 __global__ void long_fibers_k(const uint64_t *fptr, uint64_t nfib, uint32_t *list, unsigned long long *count)
 {
     GRID_LOOP(f, nfib)
-    if (fptr[f + 1] - fptr[f] > kShortFiber) list[atomicAdd(count, 1ull)] = (uint32_t)f;
+    {
+        const uint64_t len = fptr[f + 1] - fptr[f];
+        if (len > kVLongFiber) list[nfib - 1 - atomicAdd(count + 1, 1ull)] = (uint32_t)f;
+        else if (len > kShortFiber) list[atomicAdd(count, 1ull)] = (uint32_t)f;
+    }
 }
 
-// One thread per short fiber, NC4 float4 column chunks (R <= 4 * NC4 <= 32).
+// Length class of every fiber for the one-thread-per-fiber kernel: 0 for one
+// nonzero, c for 2^(c-1) < length <= 2^c up to kShortFiber, 7 above.
+__global__ void fiber_class_k(const uint64_t *fptr, uint64_t nfib, uint64_t *key, uint32_t *idx)
+{
+    GRID_LOOP(f, nfib)
+    {
+        const uint64_t len = fptr[f + 1] - fptr[f];
+        key[f] = len > kShortFiber ? 7u : (len <= 1 ? 0u : 64u - __clzll(len - 1));
+        idx[f] = (uint32_t)f;
+    }
+}
+
+// One thread per short fiber, NC4 float4 column chunks (R <= 4 * NC4 <= 32);
+// the fibers are taken in `order` (grouped by length, so that a warp's lanes
+// walk fibers of similar lengths and finish together).
 // U rows and Y rows are 16-byte aligned (ldu, ldy multiples of 4).
 template <int NC4>
-__global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restrict__ fptr, uint64_t nfib,
+__global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restrict__ fptr,
+                                                        const uint32_t *__restrict__ order, uint64_t nshort,
                                                         const uint32_t *__restrict__ sind,
                                                         const float *__restrict__ sval,
                                                         const float *__restrict__ U, uint32_t ldu,
                                                         float *__restrict__ Y, uint32_t ldy, uint32_t R)
 {
-    GRID_LOOP(f, nfib)
+    GRID_LOOP(i, nshort)
     {
+        const uint64_t f = order[i];
         const uint64_t b = fptr[f], e = fptr[f + 1];
-        if (e - b > kShortFiber) continue;
         float4 acc[NC4];
 #pragma unroll
         for (int c = 0; c < NC4; ++c) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -146,19 +176,23 @@ __global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restri
     }
 }
 
-// Long fibers (R <= 32, U rows 16-byte aligned): one warp per fiber, lane l
-// summing column l.  Two cp.async stages run ahead of the sums, in groups of
-// 32 nonzeros (lane t copying element t of a group):
-//   iteration g  copies the indices and values of group g + D into rings,
-//                copies the factor rows of group g (the indices landed D
-//                iterations ago) into the row ring,
-//                sums group g - D (its rows landed),
-// so 32 D rows are in flight per fiber while every column is summed in the
-// reference's order.  One cp.async.wait_group D-1 at the top of each
-// iteration covers both stages: everything committed at iteration g - D or
-// earlier has landed.  Dynamic shared memory: row ring (D+1) x 32 x W floats
-// (W = R rounded up to 4), index and value rings 2D+2 slots of 32.
-constexpr int kLongD = 12;
+// Long fibers (R <= 32, U rows 16-byte aligned): each warp takes fibers
+// list[blockIdx.x], list[blockIdx.x + gridDim.x], ... and walks them as one
+// stream of groups of 32 nonzeros (a fiber's last group may be shorter), lane
+// l summing column l of the current fiber.  Two cp.async stages run ahead of
+// the sums (lane t copying element t of a group):
+//   iteration g  copies the indices and values of stream group g + D into rings,
+//                copies the factor rows of stream group g (the indices landed
+//                D iterations ago) into the row ring,
+//                sums stream group g - D (its rows landed), and at the last
+//                group of a fiber writes the fiber's row of Y,
+// so 32 D rows are in flight across fiber boundaries, and the pipeline fills
+// and drains once per warp rather than once per fiber, while every column is
+// summed in the reference's order.  One cp.async.wait_group D-1 at the top of
+// each iteration covers both stages: everything committed at iteration g - D
+// or earlier has landed.  Dynamic shared memory: row ring (D+1) x 32 x W
+// floats (W = R rounded up to 4), index and value rings 2D+2 slots of 32.
+constexpr int kLongD = 6;
 constexpr int kLongRowSlots = kLongD + 1;
 constexpr int kLongIdxSlots = 2 * kLongD + 2;
 
@@ -166,6 +200,30 @@ inline size_t long_smem_bytes(uint32_t W)
 {
     return (size_t)kLongRowSlots * 32 * W * 4 + (size_t)kLongIdxSlots * 32 * 8;
 }
+
+// Position in a warp's stream of groups: fiber list[i], group k of its ng.
+struct GroupCursor {
+    uint64_t i, f, b, e, k, ng;
+    bool live;
+    __device__ __forceinline__ void fiber(const uint64_t *fptr, const uint32_t *list, uint64_t nlong)
+    {
+        live = i < nlong;
+        if (!live) return;
+        f = list[i];
+        b = fptr[f];
+        e = fptr[f + 1];
+        ng = (e - b + 31) / 32;
+        k = 0;
+    }
+    __device__ __forceinline__ void next(const uint64_t *fptr, const uint32_t *list, uint64_t nlong)
+    {
+        if (++k == ng) {
+            i += gridDim.x;
+            fiber(fptr, list, nlong);
+        }
+    }
+    __device__ __forceinline__ uint64_t first() const { return b + 32 * k; }  // first nonzero of the group
+};
 
 __global__ void __launch_bounds__(32) ttm_long_kernel(const uint64_t *__restrict__ fptr,
                                                       const uint32_t *__restrict__ list, uint64_t nlong,
@@ -184,55 +242,234 @@ __global__ void __launch_bounds__(32) ttm_long_kernel(const uint64_t *__restrict
                      "l"(src)
                      : "memory");
     };
-    for (uint64_t i = blockIdx.x; i < nlong; i += gridDim.x) {
+    // cursors of the three stages: sums (group g - D), rows (g), indices (g + D)
+    GroupCursor cs{blockIdx.x}, cr{blockIdx.x}, ci{blockIdx.x};
+    cs.fiber(fptr, list, nlong);
+    cr.fiber(fptr, list, nlong);
+    ci.fiber(fptr, list, nlong);
+    float acc = 0.f;
+    // ring slots of stream group g: row slot g mod (D+1), index slot g mod (2D+2)
+    uint32_t r13 = kLongRowSlots - kLongD % kLongRowSlots, r26 = kLongIdxSlots - kLongD;  // g = -D
+    auto wrap = [](uint32_t x, uint32_t n) { return x >= n ? x - n : x; };
+    for (int64_t g = -kLongD; cs.live; ++g) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kLongD - 1) : "memory");
+        __syncwarp();
+        if (g >= kLongD) {  // sum stream group g - D
+            const uint64_t j0 = cs.first();
+            const int cnt = (cs.e - j0) < 32 ? (int)(cs.e - j0) : 32;
+            // slots of g - D: (D+1) - D = 1 row slot ahead, 2D+2 - D index slots ahead
+            const float *rows = su + (size_t)wrap(r13 + 1, kLongRowSlots) * 32 * W;
+            const float *xs = sx + wrap(r26 + (kLongIdxSlots - kLongD), kLongIdxSlots) * 32;
+            if ((uint32_t)lane < R) {
+#pragma unroll 8
+                for (int t = 0; t < cnt; ++t) acc = __fadd_rn(acc, __fmul_rn(xs[t], rows[(size_t)t * W + lane]));
+            }
+            if (cs.k + 1 == cs.ng) {  // the fiber's last group: its row of Y
+                float *y = Y + (size_t)cs.f * ldy;
+                if ((uint32_t)lane < R) y[lane] = acc;
+                for (uint32_t k = R + lane; k < ldy; k += 32) y[k] = 0.f;
+                acc = 0.f;
+            }
+            cs.next(fptr, list, nlong);
+        }
+        if (g >= 0 && cr.live) {  // rows of stream group g
+            const uint64_t mine = cr.first() + lane;
+            if (mine < cr.e) {
+                const uint32_t r = si[r26 * 32 + lane];  // this lane's own copy
+                const float *src = U + (size_t)r * ldu;
+                float *dst = su + (size_t)r13 * 32 * W + (size_t)lane * W;
+                for (uint32_t q = 0; q < W; q += 4) {
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+                                 ::"r"((unsigned)__cvta_generic_to_shared(dst + q)), "l"(src + q)
+                                 : "memory");
+                }
+            }
+            cr.next(fptr, list, nlong);
+        }
+        if (ci.live) {  // indices and values of stream group g + D
+            const uint64_t mine = ci.first() + lane;
+            if (mine < ci.e) {
+                const uint32_t slot = wrap(r26 + kLongD, kLongIdxSlots) * 32 + lane;  // slot of g + D
+                cp4(si + slot, sind + mine);
+                cp4(sx + slot, sval + mine);
+            }
+            ci.next(fptr, list, nlong);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        __syncwarp();  // the slots read above are refilled in later iterations
+        r13 = wrap(r13 + 1, kLongRowSlots);
+        r26 = wrap(r26 + 1, kLongIdxSlots);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// The longest fibers (more than kVLongFiber nonzeros; R <= 32, U rows
+// 16-byte aligned): one CTA of kVWarps warps per fiber.  The products
+// x_j * U[i_j, c] do not depend on one another, so warps 1 .. kVWarps-1
+// compute them, rounded to FP32 as the reference rounds them, into shared
+// memory, chunk by chunk of kVChunk nonzeros, and warp 0 adds the chunks in
+// fiber order, lane c summing column c.  Every column is then the reference's
+// sequence of FP32 additions, and only that chain of dependent additions is
+// serial: the factor-row gathers of up to kVWarps-1 chunks run ahead of it.
+// Chunk q of the CTA's running count belongs to producer warp 1 + q % P
+// (P = kVWarps - 1) and its slot q % P, as use q / P of that slot: each slot
+// is filled by one warp in order and emptied by warp 0 in order, so its
+// "full" mbarrier (32 arrivals, the producer's lanes) and "empty" mbarrier
+// (32 arrivals, warp 0's lanes) are never more than one phase apart, and the
+// parity waits are exact.  Every wait is bounded by a deadline on
+// %globaltimer (kVWaitNs each); a warp that gives up sets bit 2 of the error
+// word and a shared abort flag that ends the other warps' waits, and the CTA
+// stops.
+constexpr int kVWarps = 16;
+constexpr int kVSlots = kVWarps - 1;
+constexpr int kVChunk = 64;
+constexpr uint64_t kVWaitNs = 2000000000ull;  // 2 s
+
+inline size_t vlong_smem_bytes(uint32_t W) { return (size_t)kVSlots * kVChunk * W * 4; }
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_arrive_cta(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// true once the phase of `bar` with parity `parity` has completed; false if
+// `abort` is set or kVWaitNs pass first
+__device__ __forceinline__ bool vwait(uint64_t *bar, uint32_t parity, const volatile int *abort)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t deadline = global_ns() + kVWaitNs;
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*abort) return false;
+        if ((i & 255u) == 255u && global_ns() > deadline) return false;
+    }
+}
+
+__global__ void __launch_bounds__(kVWarps * 32) ttm_vlong_kernel(const uint64_t *__restrict__ fptr,
+                                                                 const uint32_t *__restrict__ list, uint64_t nvl,
+                                                                 const uint32_t *__restrict__ sind,
+                                                                 const float *__restrict__ sval,
+                                                                 const float *__restrict__ U, uint32_t ldu, uint32_t R,
+                                                                 uint32_t W, float *__restrict__ Y, uint32_t ldy,
+                                                                 uint32_t *err)
+{
+    extern __shared__ __align__(16) float vring[];  // [kVSlots][kVChunk][W]
+    __shared__ uint64_t full[kVSlots], empty[kVSlots];
+    __shared__ int abort_flag;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kVSlots; ++k) {
+            mbar_init(&full[k], 32);
+            mbar_init(&empty[k], 32);
+        }
+        abort_flag = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto give_up = [&]() {
+        if (lane == 0) {
+            atomicOr(err, 2u);
+            abort_flag = 1;
+        }
+    };
+    uint64_t q0 = 0;  // chunks of the CTA's earlier fibers
+    for (uint64_t i = blockIdx.x; i < nvl; i += gridDim.x) {
         const uint64_t f = list[i];
         const uint64_t b = fptr[f], e = fptr[f + 1];
-        const int64_t ng = (int64_t)((e - b + 31) / 32);
-        float acc = 0.f;
-        for (int64_t g = -kLongD; g < ng + kLongD; ++g) {
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(kLongD - 1) : "memory");
-            __syncwarp();
-            const int64_t gc = g - kLongD;  // group summed now
-            if (gc >= 0) {
-                const uint64_t j0 = b + 32 * (uint64_t)gc;
-                const int cnt = (e - j0) < 32 ? (int)(e - j0) : 32;
-                const float *rows = su + (size_t)(gc % kLongRowSlots) * 32 * W;
-                const float *xs = sx + (gc % kLongIdxSlots) * 32;
-                if ((uint32_t)lane < R) {
-#pragma unroll 8
-                    for (int t = 0; t < cnt; ++t) acc = __fadd_rn(acc, __fmul_rn(xs[t], rows[(size_t)t * W + lane]));
-                }
-            }
-            if (g >= 0 && g < ng) {  // rows of group g
-                const uint64_t mine = b + 32 * (uint64_t)g + lane;
-                if (mine < e) {
-                    const uint32_t r = si[(g % kLongIdxSlots) * 32 + lane];  // this lane's own copy
-                    const float *src = U + (size_t)r * ldu;
-                    float *dst = su + (size_t)(g % kLongRowSlots) * 32 * W + (size_t)lane * W;
-                    for (uint32_t q = 0; q < W; q += 4) {
-                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
-                                     ::"r"((unsigned)__cvta_generic_to_shared(dst + q)), "l"(src + q)
-                                     : "memory");
+        const uint64_t nq = (e - b + kVChunk - 1) / kVChunk;
+        if (warp == 0) {
+            float acc = 0.f;
+            uint32_t slot = (uint32_t)(q0 % kVSlots), parity = (uint32_t)(q0 / kVSlots) & 1u;  // of chunk q0 + q
+            for (uint64_t q = 0; q < nq; ++q) {
+                if (q) {
+                    if (++slot == kVSlots) {
+                        slot = 0;
+                        parity ^= 1u;
                     }
                 }
-            }
-            const int64_t gi = g + kLongD;  // indices and values of group gi
-            if (gi >= 0 && gi < ng) {
-                const uint64_t mine = b + 32 * (uint64_t)gi + lane;
-                if (mine < e) {
-                    const int slot = (int)(gi % kLongIdxSlots) * 32 + lane;
-                    cp4(si + slot, sind + mine);
-                    cp4(sx + slot, sval + mine);
+                if (!vwait(&full[slot], parity, &abort_flag)) {
+                    give_up();
+                    return;
                 }
+                const uint64_t j0 = b + q * kVChunk;
+                const int cnt = (e - j0) < (uint64_t)kVChunk ? (int)(e - j0) : kVChunk;
+                const float *src = vring + (size_t)slot * kVChunk * W + lane;
+                if ((uint32_t)lane < R) {
+                    if (cnt == kVChunk) {
+                        // straight-line: the loads of the next 16 products are
+                        // in flight while the current 16 are added
+                        float v[16], nv[16];
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) v[t] = src[(size_t)t * W];
+#pragma unroll
+                        for (int t0 = 0; t0 < kVChunk; t0 += 16) {
+                            if (t0 + 16 < kVChunk) {
+#pragma unroll
+                                for (int t = 0; t < 16; ++t) nv[t] = src[(size_t)(t0 + 16 + t) * W];
+                            }
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) acc = __fadd_rn(acc, v[t]);
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) v[t] = nv[t];
+                        }
+                    } else {
+                        for (int t = 0; t < cnt; ++t) acc = __fadd_rn(acc, src[(size_t)t * W]);
+                    }
+                }
+                mbar_arrive_cta(&empty[slot]);
             }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            __syncwarp();  // the slots read above are refilled in later iterations
+            float *y = Y + (size_t)f * ldy;
+            if ((uint32_t)lane < R) y[lane] = acc;
+            for (uint32_t k = R + lane; k < ldy; k += 32) y[k] = 0.f;
+        } else {
+            const uint64_t pw = (uint64_t)warp - 1;  // this warp's slot
+            const uint64_t qf = (pw + kVSlots - q0 % kVSlots) % kVSlots;  // its first chunk of the fiber
+            uint32_t parity = (uint32_t)((q0 + qf) / kVSlots) & 1u;      // use (q0 + q) / kVSlots of the slot
+            for (uint64_t q = qf; q < nq; q += kVSlots, parity ^= 1u) {
+                // the slot's previous chunk has been added (a fresh barrier
+                // passes the wait on the phase before its first at once)
+                if (!vwait(&empty[pw], parity ^ 1u, &abort_flag)) {
+                    give_up();
+                    return;
+                }
+                const uint64_t j0 = b + q * kVChunk;
+                const int cnt = (e - j0) < (uint64_t)kVChunk ? (int)(e - j0) : kVChunk;
+                float *dst = vring + (size_t)pw * kVChunk * W;
+                static_assert(kVChunk == 64, "two nonzeros per lane");
+                // both nonzeros' indices, then both rows, are in flight together
+                const bool h0 = lane < cnt, h1 = lane + 32 < cnt;
+                const uint32_t k0 = h0 ? sind[j0 + lane] : 0u, k1 = h1 ? sind[j0 + lane + 32] : 0u;
+                const float x0 = h0 ? sval[j0 + lane] : 0.f, x1 = h1 ? sval[j0 + lane + 32] : 0.f;
+                const float4 *u0 = reinterpret_cast<const float4 *>(U + (size_t)k0 * ldu);
+                const float4 *u1 = reinterpret_cast<const float4 *>(U + (size_t)k1 * ldu);
+                float4 *d0 = reinterpret_cast<float4 *>(dst + (size_t)lane * W);
+                float4 *d1 = reinterpret_cast<float4 *>(dst + (size_t)(lane + 32) * W);
+                float4 v0[8], v1[8];  // W <= 32: at most 8 float4 per row
+#pragma unroll
+                for (uint32_t c = 0; c < 8; ++c) {
+                    v0[c] = h0 && c < W / 4 ? __ldg(u0 + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    v1[c] = h1 && c < W / 4 ? __ldg(u1 + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (uint32_t c = 0; c < 8; ++c) {
+                    if (h0 && c < W / 4)
+                        d0[c] = make_float4(__fmul_rn(x0, v0[c].x), __fmul_rn(x0, v0[c].y), __fmul_rn(x0, v0[c].z),
+                                            __fmul_rn(x0, v0[c].w));
+                    if (h1 && c < W / 4)
+                        d1[c] = make_float4(__fmul_rn(x1, v1[c].x), __fmul_rn(x1, v1[c].y), __fmul_rn(x1, v1[c].z),
+                                            __fmul_rn(x1, v1[c].w));
+                }
+                mbar_arrive_cta(&full[pw]);
+            }
         }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-        float *y = Y + (size_t)f * ldy;
-        if ((uint32_t)lane < R) y[lane] = acc;
-        for (uint32_t k = R + lane; k < ldy; k += 32) y[k] = 0.f;
-        __syncwarp();
+        q0 += nq;
     }
 }
 
@@ -387,19 +624,34 @@ int fiber_plan(ptiB200Tensor *t, uint32_t mode, bool sort, cudaStream_t s)
     // fibers too long for one thread each (their order in the list is free:
     // every fiber is computed on its own)
     DevBuf cnt;
-    PTI_CUDA(cnt.alloc(padded(8), s), mod);
-    PTI_CUDA(cudaMemsetAsync(cnt.ptr, 0, 8, s), mod);
+    PTI_CUDA(cnt.alloc(padded(16), s), mod);
+    PTI_CUDA(cudaMemsetAsync(cnt.ptr, 0, 16, s), mod);
     PTI_CUDA(P.long_fibers.alloc(padded(nfib * 4), s), mod);
-    unsigned long long nlong = 0;
+    unsigned long long nlong[2] = {0, 0};
     if (nfib) {
         long_fibers_k<<<grid_t(nfib), 256, 0, s>>>(P.fptr.as<uint64_t>(), nfib, P.long_fibers.as<uint32_t>(),
                                                   cnt.as<unsigned long long>());
-        PTI_CUDA(cudaMemcpyAsync(&nlong, cnt.ptr, 8, cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaMemcpyAsync(nlong, cnt.ptr, 16, cudaMemcpyDeviceToHost, s), mod);
         PTI_CUDA(cudaStreamSynchronize(s), mod);
     }
     PTI_CUDA(cudaGetLastError(), mod);
     P.nfib = nfib;
-    P.nlong = nlong;
+    P.nlong = nlong[0];
+    P.nvlong = nlong[1];
+    // the fibers one thread takes, by length class (a stable sort of the
+    // classes, so fibers of one class stay in fiber order)
+    P.nshort = nfib - P.nlong - P.nvlong;
+    if (nfib) {
+        DevBuf keys;
+        RadixScratch rs;
+        PTI_CUDA(keys.alloc(padded(nfib * 8), s), mod);
+        PTI_CUDA(P.short_order.alloc(padded(nfib * 4), s), mod);
+        PTI_TRY(rs.alloc(nfib, s));
+        fiber_class_k<<<grid_t(nfib), 256, 0, s>>>(P.fptr.as<uint64_t>(), nfib, keys.as<uint64_t>(),
+                                                    P.short_order.as<uint32_t>());
+        PTI_TRY(radix_sort_pairs(keys, P.short_order, nfib, 3, rs, s));
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+    }
     P.ready = true;
     return 0;
 }
@@ -431,44 +683,69 @@ int ttm_device(ptiB200Tensor *t, uint32_t mode, const float *U, uint32_t R, uint
                             reinterpret_cast<uintptr_t>(U) % 16 == 0 && reinterpret_cast<uintptr_t>(Y) % 16 == 0;
     uint64_t ngroup = P.nfib;
     const uint32_t *list = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaEvent_t ev[1] = {nullptr};
     bool joined = true;
-    if (short_path && P.nlong) {
-        // the long fibers run beside the short ones, on a second stream
+    cudaEvent_t ev_vl = nullptr, ev_l = nullptr;
+    if (short_path && (P.nlong || P.nvlong)) {
+        // the long fibers run beside the short ones: the longest (whose serial
+        // sums are the longest chains) on one side stream, the others on a
+        // second, so that neither waits for the other
         const uint32_t W = 4 * nc4;
-        const size_t smem = long_smem_bytes(W);
-        PTI_CUDA(cudaFuncSetAttribute(ttm_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                 mod);
-        cudaStream_t s2 = copy_stream();
         PTI_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), mod);
-        PTI_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), mod);
         PTI_CUDA(cudaEventRecord(ev[0], s), mod);
-        PTI_CUDA(cudaStreamWaitEvent(s2, ev[0], 0), mod);
-        const unsigned grid = (unsigned)std::min<uint64_t>(P.nlong, (uint64_t)sms * 8);
-        ttm_long_kernel<<<grid, 32, smem, s2>>>(fp, P.long_fibers.as<uint32_t>(), P.nlong, si, sv, U, ldu, R, W, Y,
-                                                ldy);
-        PTI_CUDA(cudaGetLastError(), mod);
-        PTI_CUDA(cudaEventRecord(ev[1], s2), mod);
+        if (P.nvlong) {
+            cudaStream_t s2 = side_stream(0);
+            PTI_CUDA(cudaStreamWaitEvent(s2, ev[0], 0), mod);
+            PTI_TRY(ensure_err_word(t, s2));
+            const size_t smem = vlong_smem_bytes(W);
+            PTI_CUDA(cudaFuncSetAttribute(ttm_vlong_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                     mod);
+            const unsigned grid = (unsigned)std::min<uint64_t>(P.nvlong, (uint64_t)sms * 2);
+            ttm_vlong_kernel<<<grid, kVWarps * 32, smem, s2>>>(fp, P.long_fibers.as<uint32_t>() + (P.nfib - P.nvlong),
+                                                               P.nvlong, si, sv, U, ldu, R, W, Y, ldy, err_word(t));
+            PTI_CUDA(cudaGetLastError(), mod);
+            PTI_CUDA(cudaEventCreateWithFlags(&ev_vl, cudaEventDisableTiming), mod);
+            PTI_CUDA(cudaEventRecord(ev_vl, s2), mod);
+        }
+        if (P.nlong) {
+            cudaStream_t s3 = side_stream(1);
+            PTI_CUDA(cudaStreamWaitEvent(s3, ev[0], 0), mod);
+            const size_t smem = long_smem_bytes(W);
+            PTI_CUDA(cudaFuncSetAttribute(ttm_long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                     mod);
+            const unsigned grid = (unsigned)std::min<uint64_t>(P.nlong, (uint64_t)sms * 8);
+            ttm_long_kernel<<<grid, 32, smem, s3>>>(fp, P.long_fibers.as<uint32_t>(), P.nlong, si, sv, U, ldu, R, W,
+                                                    Y, ldy);
+            PTI_CUDA(cudaGetLastError(), mod);
+            PTI_CUDA(cudaEventCreateWithFlags(&ev_l, cudaEventDisableTiming), mod);
+            PTI_CUDA(cudaEventRecord(ev_l, s3), mod);
+        }
         joined = false;
     }
     if (short_path) {
-        const unsigned g = grid_t(P.nfib);
-        switch (nc4) {
-        case 1: ttm_short_kernel<1><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 2: ttm_short_kernel<2><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 3: ttm_short_kernel<3><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 4: ttm_short_kernel<4><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 5: ttm_short_kernel<5><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 6: ttm_short_kernel<6><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        case 7: ttm_short_kernel<7><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
-        default: ttm_short_kernel<8><<<g, 256, 0, s>>>(fp, P.nfib, si, sv, U, ldu, Y, ldy, R); break;
+        // a thread per fiber and as many CTAs as that takes: CTAs finish in
+        // turn, so the long-fiber kernels beside this one find room
+        const unsigned g = (unsigned)std::max<uint64_t>(1, (P.nshort + 255) / 256);
+        const uint32_t *so = P.short_order.as<uint32_t>();
+        const uint64_t ns = P.nshort;
+        if (ns) switch (nc4) {
+        case 1: ttm_short_kernel<1><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 2: ttm_short_kernel<2><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 3: ttm_short_kernel<3><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 4: ttm_short_kernel<4><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 5: ttm_short_kernel<5><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 6: ttm_short_kernel<6><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 7: ttm_short_kernel<7><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        default: ttm_short_kernel<8><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
         }
         ngroup = 0;  // the long fibers are on the second stream
     }
     if (!joined) {  // `s` continues once the long fibers are done too
-        PTI_CUDA(cudaStreamWaitEvent(s, ev[1], 0), mod);
+        if (ev_vl) PTI_CUDA(cudaStreamWaitEvent(s, ev_vl, 0), mod);
+        if (ev_l) PTI_CUDA(cudaStreamWaitEvent(s, ev_l, 0), mod);
         cudaEventDestroy(ev[0]);
-        cudaEventDestroy(ev[1]);
+        if (ev_vl) cudaEventDestroy(ev_vl);
+        if (ev_l) cudaEventDestroy(ev_l);
     }
     if (ngroup) {
         const int G = R > 16 ? 32 : (R > 8 ? 16 : 8);
@@ -578,7 +855,7 @@ int host_ttm(ptiSemiSparseTensor *Y, ptiSparseTensor *X, const ptiValue *Uvals, 
     if (nfib)
         PTI_CUDA(cudaMemcpyAsync(Y->values.values, dY.ptr, nfib * stride * 4, cudaMemcpyDeviceToHost, s), mod);
     PTI_CUDA(cudaStreamSynchronize(s), mod);
-    return 0;
+    return take_device_error(&t, s, mod);
 }
 
 // ---------------------------------------------------------------------------

@@ -151,3 +151,20 @@ def test_semi_sparse_ttm_matches_reference(lib, cuda, ref, R2):
     for a, b in zip(got["inds"], want_inds):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(got["vals"].view(np.uint32), want_vals.view(np.uint32))
+
+
+@pytest.mark.parametrize("dims,nnz,R", [((20000, 4, 3), 150_000, 16), ((20000, 4, 3), 150_000, 5),
+                                        ((30000, 3, 2), 120_000, 32), ((10000, 40, 10), 3_600_000, 16)])
+def test_ttm_very_long_fibers_match_reference(lib, cuda, ref, dims, nnz, R):
+    """Fibers of more than 8192 nonzeros along mode 0 (one CTA per fiber: the
+    products computed by producer warps, the column sums added by one warp in
+    fiber order), mixed with shorter fibers along the other modes; the last
+    case has 400 such fibers, more than the grid, so CTAs take several.  Bit
+    for bit against the reference's ptiSparseTensorMulMatrix."""
+    inds, vals = _tensor(dims, nnz, R + 7)
+    rng = np.random.default_rng(R)
+    for mode in range(3):
+        U = rng.standard_normal((dims[mode], R)).astype(np.float32)
+        theirs = ref.ttm(dims, inds, vals, U, mode)
+        coo = COOTensor(dims, [i.copy() for i in inds], vals.copy())
+        _check(coo.ttm(U, mode), theirs, coo, mode)
