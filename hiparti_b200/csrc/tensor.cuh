@@ -54,7 +54,7 @@ struct FiberPlan {
     uint64_t nlong = 0;                    // fibers longer than one thread takes, up to the CTA limit
     uint64_t nvlong = 0;                   // fibers longer than that, one CTA each
     uint64_t nshort = 0;                   // fibers one thread takes
-    DevBuf short_order;                    // uint32 [nfib]: those nshort fibers first, by length class
+    DevBuf short_fibs;                     // uint4 [nshort]: {fiber, length, first nonzero} by length class
     DevBuf long_fibers;                    // uint32 [nfib]: the nlong fibers from the front, the nvlong from the back
 };
 

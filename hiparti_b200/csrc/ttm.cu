@@ -124,13 +124,24 @@ __global__ void fiber_class_k(const uint64_t *fptr, uint64_t nfib, uint64_t *key
     }
 }
 
-// One thread per short fiber, NC4 float4 column chunks (R <= 4 * NC4 <= 32);
-// the fibers are taken in `order` (grouped by length, so that a warp's lanes
-// walk fibers of similar lengths and finish together).
+// {fiber, length, first nonzero} of the fibers in `order`, for the kernel below.
+__global__ void pack_short_k(const uint64_t *fptr, const uint32_t *order, uint64_t n, uint4 *fibs)
+{
+    GRID_LOOP(i, n)
+    {
+        const uint32_t f = order[i];
+        const uint64_t b = fptr[f];
+        fibs[i] = make_uint4(f, (uint32_t)(fptr[f + 1] - b), (uint32_t)b, (uint32_t)(b >> 32));
+    }
+}
+
+// One thread per short fiber, NC4 float4 column chunks (R <= 4 * NC4 <= 32).
+// The fibers come packed in order of their length class (so that a warp's
+// lanes walk fibers of similar lengths and finish together), each with its
+// first nonzero, so a thread starts from one coalesced 16-byte load.
 // U rows and Y rows are 16-byte aligned (ldu, ldy multiples of 4).
 template <int NC4>
-__global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restrict__ fptr,
-                                                        const uint32_t *__restrict__ order, uint64_t nshort,
+__global__ void __launch_bounds__(256) ttm_short_kernel(const uint4 *__restrict__ fibs, uint64_t nshort,
                                                         const uint32_t *__restrict__ sind,
                                                         const float *__restrict__ sval,
                                                         const float *__restrict__ U, uint32_t ldu,
@@ -138,8 +149,9 @@ __global__ void __launch_bounds__(256) ttm_short_kernel(const uint64_t *__restri
 {
     GRID_LOOP(i, nshort)
     {
-        const uint64_t f = order[i];
-        const uint64_t b = fptr[f], e = fptr[f + 1];
+        const uint4 fb = fibs[i];  // {fiber, length, first nonzero (64-bit)}
+        const uint64_t f = fb.x;
+        const uint64_t b = (uint64_t)fb.z | (uint64_t)fb.w << 32, e = b + fb.y;
         float4 acc[NC4];
 #pragma unroll
         for (int c = 0; c < NC4; ++c) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -641,15 +653,18 @@ int fiber_plan(ptiB200Tensor *t, uint32_t mode, bool sort, cudaStream_t s)
     // the fibers one thread takes, by length class (a stable sort of the
     // classes, so fibers of one class stay in fiber order)
     P.nshort = nfib - P.nlong - P.nvlong;
-    if (nfib) {
-        DevBuf keys;
+    if (P.nshort) {
+        DevBuf keys, order;
         RadixScratch rs;
         PTI_CUDA(keys.alloc(padded(nfib * 8), s), mod);
-        PTI_CUDA(P.short_order.alloc(padded(nfib * 4), s), mod);
+        PTI_CUDA(order.alloc(padded(nfib * 4), s), mod);
         PTI_TRY(rs.alloc(nfib, s));
         fiber_class_k<<<grid_t(nfib), 256, 0, s>>>(P.fptr.as<uint64_t>(), nfib, keys.as<uint64_t>(),
-                                                    P.short_order.as<uint32_t>());
-        PTI_TRY(radix_sort_pairs(keys, P.short_order, nfib, 3, rs, s));
+                                                    order.as<uint32_t>());
+        PTI_TRY(radix_sort_pairs(keys, order, nfib, 3, rs, s));
+        PTI_CUDA(P.short_fibs.alloc(padded(P.nshort * 16), s), mod);
+        pack_short_k<<<grid_t(P.nshort), 256, 0, s>>>(P.fptr.as<uint64_t>(), order.as<uint32_t>(), P.nshort,
+                                                       P.short_fibs.as<uint4>());
         PTI_CUDA(cudaStreamSynchronize(s), mod);
     }
     P.ready = true;
@@ -726,17 +741,17 @@ int ttm_device(ptiB200Tensor *t, uint32_t mode, const float *U, uint32_t R, uint
         // a thread per fiber and as many CTAs as that takes: CTAs finish in
         // turn, so the long-fiber kernels beside this one find room
         const unsigned g = (unsigned)std::max<uint64_t>(1, (P.nshort + 255) / 256);
-        const uint32_t *so = P.short_order.as<uint32_t>();
+        const uint4 *sf = P.short_fibs.as<uint4>();
         const uint64_t ns = P.nshort;
         if (ns) switch (nc4) {
-        case 1: ttm_short_kernel<1><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 2: ttm_short_kernel<2><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 3: ttm_short_kernel<3><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 4: ttm_short_kernel<4><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 5: ttm_short_kernel<5><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 6: ttm_short_kernel<6><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        case 7: ttm_short_kernel<7><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
-        default: ttm_short_kernel<8><<<g, 256, 0, s>>>(fp, so, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 1: ttm_short_kernel<1><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 2: ttm_short_kernel<2><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 3: ttm_short_kernel<3><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 4: ttm_short_kernel<4><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 5: ttm_short_kernel<5><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 6: ttm_short_kernel<6><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        case 7: ttm_short_kernel<7><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
+        default: ttm_short_kernel<8><<<g, 256, 0, s>>>(sf, ns, si, sv, U, ldu, Y, ldy, R); break;
         }
         ngroup = 0;  // the long fibers are on the second stream
     }
