@@ -449,24 +449,35 @@ int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s
         PTI_CUDA(t->einds[m].alloc(padded(t->nnz), s), mod);
     }
     PTI_CUDA(t->vals.alloc(padded(t->nnz * 4), s), mod);
-    if (s2) {  // s2 may use the buffers once their stream-ordered allocation is done
+    auto copy_mode = [&](uint32_t m, cudaStream_t cs) -> int {
+        if (t->nb)
+            PTI_CUDA(cudaMemcpyAsync(t->binds[m].ptr, H->binds[m].data, t->nb * 4, cudaMemcpyHostToDevice, cs), mod);
+        if (t->nnz)
+            PTI_CUDA(cudaMemcpyAsync(t->einds[m].ptr, H->einds[m].data, t->nnz, cudaMemcpyHostToDevice, cs), mod);
+        return 0;
+    };
+    PTI_CUDA(cudaMemcpyAsync(t->bptr.ptr, H->bptr.data, (t->nb + 1) * 8, cudaMemcpyHostToDevice, s), mod);
+    if (s2) {
+        // The arrays the schedule starts from go first, alone on the host
+        // link; the rest starts on s2 when they have landed (and the buffers'
+        // stream-ordered allocations are done), so it overlaps the schedule
+        // build instead of slowing down its inputs.
+        if (first_mode >= 0) PTI_TRY(copy_mode((uint32_t)first_mode, s));
         cudaEvent_t ev;
         PTI_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), mod);
         cudaEventRecord(ev, s);
         cudaStreamWaitEvent(s2, ev, 0);
         cudaEventDestroy(ev);
-    }
-    PTI_CUDA(cudaMemcpyAsync(t->bptr.ptr, H->bptr.data, (t->nb + 1) * 8, cudaMemcpyHostToDevice, s), mod);
-    for (uint32_t m = 0; m < H->nmodes; ++m) {
-        cudaStream_t cs = s2 && (int)m != first_mode ? s2 : s;
-        if (t->nb)
-            PTI_CUDA(cudaMemcpyAsync(t->binds[m].ptr, H->binds[m].data, t->nb * 4, cudaMemcpyHostToDevice, cs), mod);
         if (t->nnz)
-            PTI_CUDA(cudaMemcpyAsync(t->einds[m].ptr, H->einds[m].data, t->nnz, cudaMemcpyHostToDevice, cs), mod);
+            PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s2), mod);
+        for (uint32_t m = 0; m < H->nmodes; ++m)
+            if ((int)m != first_mode) PTI_TRY(copy_mode(m, s2));
+        if (late) PTI_CUDA(cudaEventRecord(late, s2), mod);
+    } else {
+        for (uint32_t m = 0; m < H->nmodes; ++m) PTI_TRY(copy_mode(m, s));
+        if (t->nnz)
+            PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s), mod);
     }
-    if (t->nnz)
-        PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s2 ? s2 : s), mod);
-    if (s2 && late) PTI_CUDA(cudaEventRecord(late, s2), mod);
     PTI_TRY(ensure_err_word(t, s));
     if (t->nb) {
         check_bptr_kernel<<<grid_for(t->nb + 1, 256), 256, 0, s>>>(t->bptr.as<uint64_t>(), t->nb, t->nnz,
@@ -498,21 +509,26 @@ int check_mats(uint32_t N, const uint32_t *ndims, ptiMatrix **mats, const char *
     return 0;
 }
 
+// With s2 and late (the tensor's remaining arrays being copied on s2), the
+// factors are copied on s2 behind them and `late` is recorded again after
+// them: the schedule build on s does not wait for the factors, the kernel does.
 int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, ptiIndex mode,
-             cudaStream_t s, const char *mod, cudaEvent_t late = nullptr)
+             cudaStream_t s, const char *mod, cudaEvent_t late = nullptr, cudaStream_t s2 = nullptr)
 {
     const uint32_t N = t->nmodes;
     const uint32_t R = mats[mode]->ncols, stride = mats[0]->stride;
     PTI_CHECK(mats[N]->cap >= t->ndims[mode], PTIERR_SHAPE_MISMATCH, mod, "mats[nmodes] has too few rows");
     DevBuf dm[kMaxModes], dout;
     const void *ptrs[kMaxModes] = {nullptr};
+    const cudaStream_t fs = s2 && late ? s2 : s;
     for (uint32_t k = 0; k < N; ++k) {
         if (k == mode) continue;
         size_t bytes = (size_t)t->ndims[k] * stride * 4;
-        PTI_CUDA(dm[k].alloc(padded(bytes), s), mod);
-        PTI_CUDA(cudaMemcpyAsync(dm[k].ptr, mats[k]->values, bytes, cudaMemcpyHostToDevice, s), mod);
+        PTI_CUDA(dm[k].alloc(padded(bytes), fs), mod);
+        PTI_CUDA(cudaMemcpyAsync(dm[k].ptr, mats[k]->values, bytes, cudaMemcpyHostToDevice, fs), mod);
         ptrs[k] = dm[k].ptr;
     }
+    if (fs != s) PTI_CUDA(cudaEventRecord(late, s2), mod);
     size_t obytes = (size_t)t->ndims[mode] * stride * 4;
     PTI_CUDA(dout.alloc(padded(obytes), s), mod);
     PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s, nullptr, late));
@@ -549,7 +565,7 @@ int mttkrp_host_hicoo(const ptiSparseTensorHiCOO *H, ptiMatrix **mats, const pti
     {
         ptiB200Tensor t;
         r = upload_hicoo(&t, H, s, (int)mode, s2, late);
-        if (r == 0) r = run_host(&t, mats, mats_order, mode, s, mod, late);
+        if (r == 0) r = run_host(&t, mats, mats_order, mode, s, mod, late, s2);
         cudaStreamWaitEvent(s, late, 0);  // the tensor is released on s only after the second stream's copies
     }
     cudaEventDestroy(late);
