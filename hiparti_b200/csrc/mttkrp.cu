@@ -239,7 +239,7 @@ static bool use_schedule(const ptiB200Tensor *t, uint32_t R, uint32_t stride)
 
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                   const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s, const float *vals_override,
-                  cudaEvent_t late)
+                  const Arrivals *arr)
 {
     const char *mod = "B200 MTTKRP";
     const uint32_t N = t->nmodes;
@@ -268,11 +268,11 @@ int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R,
     if (t->nnz == 0) return 0;
     const int G = group_lanes(R);
     if (use_schedule(t, R, stride)) {
-        PTI_TRY(prepare_mode(t, mode, s, late));
-        if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
+        PTI_TRY(prepare_mode(t, mode, s, arr));
+        if (arr && arr->all) PTI_CUDA(cudaStreamWaitEvent(s, arr->all, 0), mod);
         return mttkrp_scheduled(t, mats, ft, R, stride, mats_order, mode, out, s, vals_override);
     }
-    if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
+    if (arr && arr->all) PTI_CUDA(cudaStreamWaitEvent(s, arr->all, 0), mod);
 
     if (!t->hicoo) {
         CooArgs a{};
@@ -421,7 +421,7 @@ int finish_hicoo_layout(ptiB200Tensor *t, cudaStream_t s)
 }
 
 int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s, int first_mode, cudaStream_t s2,
-                 cudaEvent_t late)
+                 Arrivals *arr)
 {
     const char *mod = "B200 Upload";
     PTI_CHECK(H && H->nmodes >= 2 && H->nmodes <= (uint32_t)kMaxModes, PTIERR_VALUE_ERROR, mod,
@@ -470,9 +470,13 @@ int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s
         cudaEventDestroy(ev);
         if (t->nnz)
             PTI_CUDA(cudaMemcpyAsync(t->vals.ptr, H->values.data, t->nnz * 4, cudaMemcpyHostToDevice, s2), mod);
+        if (arr && arr->vals) PTI_CUDA(cudaEventRecord(arr->vals, s2), mod);
         for (uint32_t m = 0; m < H->nmodes; ++m)
-            if ((int)m != first_mode) PTI_TRY(copy_mode(m, s2));
-        if (late) PTI_CUDA(cudaEventRecord(late, s2), mod);
+            if ((int)m != first_mode) {
+                PTI_TRY(copy_mode(m, s2));
+                if (arr && arr->mode[m]) PTI_CUDA(cudaEventRecord(arr->mode[m], s2), mod);
+            }
+        if (arr && arr->all) PTI_CUDA(cudaEventRecord(arr->all, s2), mod);
     } else {
         for (uint32_t m = 0; m < H->nmodes; ++m) PTI_TRY(copy_mode(m, s));
         if (t->nnz)
@@ -509,18 +513,18 @@ int check_mats(uint32_t N, const uint32_t *ndims, ptiMatrix **mats, const char *
     return 0;
 }
 
-// With s2 and late (the tensor's remaining arrays being copied on s2), the
-// factors are copied on s2 behind them and `late` is recorded again after
+// With s2 and arr (the tensor's remaining arrays being copied on s2), the
+// factors are copied on s2 behind them and arr->all is recorded again after
 // them: the schedule build on s does not wait for the factors, the kernel does.
 int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, ptiIndex mode,
-             cudaStream_t s, const char *mod, cudaEvent_t late = nullptr, cudaStream_t s2 = nullptr)
+             cudaStream_t s, const char *mod, Arrivals *arr = nullptr, cudaStream_t s2 = nullptr)
 {
     const uint32_t N = t->nmodes;
     const uint32_t R = mats[mode]->ncols, stride = mats[0]->stride;
     PTI_CHECK(mats[N]->cap >= t->ndims[mode], PTIERR_SHAPE_MISMATCH, mod, "mats[nmodes] has too few rows");
     DevBuf dm[kMaxModes], dout;
     const void *ptrs[kMaxModes] = {nullptr};
-    const cudaStream_t fs = s2 && late ? s2 : s;
+    const cudaStream_t fs = s2 && arr && arr->all ? s2 : s;
     for (uint32_t k = 0; k < N; ++k) {
         if (k == mode) continue;
         size_t bytes = (size_t)t->ndims[k] * stride * 4;
@@ -528,10 +532,10 @@ int run_host(ptiB200Tensor *t, ptiMatrix **mats, const ptiIndex *mats_order, pti
         PTI_CUDA(cudaMemcpyAsync(dm[k].ptr, mats[k]->values, bytes, cudaMemcpyHostToDevice, fs), mod);
         ptrs[k] = dm[k].ptr;
     }
-    if (fs != s) PTI_CUDA(cudaEventRecord(late, s2), mod);
+    if (fs != s) PTI_CUDA(cudaEventRecord(arr->all, s2), mod);
     size_t obytes = (size_t)t->ndims[mode] * stride * 4;
     PTI_CUDA(dout.alloc(padded(obytes), s), mod);
-    PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s, nullptr, late));
+    PTI_TRY(mttkrp_device(t, ptrs, PTI_B200_F32, R, stride, mats_order, mode, dout.as<float>(), s, nullptr, arr));
     PTI_CUDA(cudaMemcpyAsync(mats[N]->values, dout.ptr, obytes, cudaMemcpyDeviceToHost, s), mod);
     PTI_TRY(take_device_error(t, s, mod));
     return 0;
@@ -559,16 +563,26 @@ int mttkrp_host_hicoo(const ptiSparseTensorHiCOO *H, ptiMatrix **mats, const pti
     // mode's coordinates and offsets) are copied first on s; the rest follows
     // on a second stream while the schedule is being built.
     cudaStream_t s = sync_stream(), s2 = copy_stream();
-    cudaEvent_t late = nullptr;
-    PTI_CUDA(cudaEventCreateWithFlags(&late, cudaEventDisableTiming), mod);
-    int r;
+    Arrivals arr;
+    int r = 0;
+    auto make = [&](cudaEvent_t *ev) {
+        if (r == 0 && cudaEventCreateWithFlags(ev, cudaEventDisableTiming) != cudaSuccess) r = PTIERR_CUDA_ERROR;
+    };
+    make(&arr.all);
+    make(&arr.vals);
+    for (uint32_t m = 0; m < H->nmodes && m < (uint32_t)kMaxModes; ++m)
+        if (m != mode) make(&arr.mode[m]);
+    PTI_CHECK(r == 0, r, mod, "event creation failed");
     {
         ptiB200Tensor t;
-        r = upload_hicoo(&t, H, s, (int)mode, s2, late);
-        if (r == 0) r = run_host(&t, mats, mats_order, mode, s, mod, late, s2);
-        cudaStreamWaitEvent(s, late, 0);  // the tensor is released on s only after the second stream's copies
+        r = upload_hicoo(&t, H, s, (int)mode, s2, &arr);
+        if (r == 0) r = run_host(&t, mats, mats_order, mode, s, mod, &arr, s2);
+        cudaStreamWaitEvent(s, arr.all, 0);  // the tensor is released on s only after the second stream's copies
     }
-    cudaEventDestroy(late);
+    cudaEventDestroy(arr.all);
+    cudaEventDestroy(arr.vals);
+    for (uint32_t m = 0; m < (uint32_t)kMaxModes; ++m)
+        if (arr.mode[m]) cudaEventDestroy(arr.mode[m]);
     return r;
 }
 

@@ -645,7 +645,7 @@ static unsigned grid_n(uint64_t n)
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 32));
 }
 
-int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, cudaEvent_t late)
+int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals *arr)
 {
     const char *mod = "B200 Prepare";
     PTI_CHECK(mode < t->nmodes, PTIERR_VALUE_ERROR, mod, "mode out of range");
@@ -731,25 +731,34 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, cudaEvent_t la
                                                   order.as<uint32_t>());
         border.reset();
         // 4. everything up to here read only bptr and the output mode's arrays;
-        // the gathers below read every array
-        if (late) PTI_CUDA(cudaStreamWaitEvent(s, late, 0), mod);
-        for (uint32_t k = 0; k < N; ++k) {
-            PTI_CUDA(P.binds[k].alloc(padded(nb * 4), s), mod);
-            gather_kernel<uint32_t><<<grid_n(nb), 256, 0, s>>>(t->binds[k].as<uint32_t>(), bperm.as<uint32_t>(), nb,
-                                                               P.binds[k].as<uint32_t>());
-        }
-        bperm.reset();
-        for (uint32_t k = 0; k < N; ++k) {
-            PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
-            gather_kernel<uint8_t><<<grid_n(n), 256, 0, s>>>(t->einds[k].as<uint8_t>(), order.as<uint32_t>(), n,
-                                                             P.einds[k].as<uint8_t>());
-        }
-        PTI_CUDA(P.vals.alloc(padded(n * 4), s), mod);
-        gather_kernel<float><<<grid_n(n), 256, 0, s>>>(t->vals.as<float>(), order.as<uint32_t>(), n,
-                                                       P.vals.as<float>());
+        // the gathers below read every array, each after its own arrival
+        // (with `arr`), in the order the arrays arrive: the output mode's,
+        // the values, then the other modes
         PTI_CUDA(P.lblk.alloc(padded(n * 2), s), mod);
         local_block_kernel<<<grid_n(n), 256, 0, s>>>(order.as<uint32_t>(), n, blk.as<uint32_t>(), inv.as<uint32_t>(),
                                                      P.tile_block.as<uint32_t>(), P.lblk.as<uint16_t>());
+        auto wait = [&](cudaEvent_t ev) -> int {
+            if (ev) PTI_CUDA(cudaStreamWaitEvent(s, ev, 0), mod);
+            return 0;
+        };
+        auto gather_mode = [&](uint32_t k) -> int {
+            if (arr) PTI_TRY(wait(arr->mode[k]));
+            PTI_CUDA(P.binds[k].alloc(padded(nb * 4), s), mod);
+            gather_kernel<uint32_t><<<grid_n(nb), 256, 0, s>>>(t->binds[k].as<uint32_t>(), bperm.as<uint32_t>(), nb,
+                                                               P.binds[k].as<uint32_t>());
+            PTI_CUDA(P.einds[k].alloc(padded(n), s), mod);
+            gather_kernel<uint8_t><<<grid_n(n), 256, 0, s>>>(t->einds[k].as<uint8_t>(), order.as<uint32_t>(), n,
+                                                             P.einds[k].as<uint8_t>());
+            return 0;
+        };
+        PTI_TRY(gather_mode(mode));
+        if (arr) PTI_TRY(wait(arr->vals));
+        PTI_CUDA(P.vals.alloc(padded(n * 4), s), mod);
+        gather_kernel<float><<<grid_n(n), 256, 0, s>>>(t->vals.as<float>(), order.as<uint32_t>(), n,
+                                                       P.vals.as<float>());
+        for (uint32_t k = 0; k < N; ++k)
+            if (k != mode) PTI_TRY(gather_mode(k));
+        bperm.reset();
     }
     inv.reset();
     PTI_CUDA(cudaGetLastError(), mod);

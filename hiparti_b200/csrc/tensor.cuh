@@ -89,6 +89,16 @@ struct ptiB200Tensor {
 
 namespace pti {
 
+// Events marking when a HiCOO tensor's arrays reach the device, for a
+// schedule built while its copies still run (the drop-in HiCOO MTTKRP): each
+// gather of the schedule waits only for its own array.  A null event means
+// the array is already ordered before the caller's stream.
+struct Arrivals {
+    cudaEvent_t mode[kMaxModes] = {};  // binds[m] and einds[m]
+    cudaEvent_t vals = nullptr;
+    cudaEvent_t all = nullptr;         // everything the kernel reads, the factors included
+};
+
 int upload_coo(ptiB200Tensor *t, const ptiSparseTensor *X, cudaStream_t s);
 // Checks every index of a device COO tensor against the mode sizes.
 int check_coo_ranges(ptiB200Tensor *t, cudaStream_t s);
@@ -98,21 +108,21 @@ int ingest_file(ptiB200Tensor *t, uint32_t start_index, const char *fname, bool 
 // Sorts t's nonzeros by coordinate and merges repeated coordinates.
 int dedupe_coo(ptiB200Tensor *t, cudaStream_t s);
 // With s2, the arrays that mode first_mode's schedule does not need first
-// (the other modes' coordinates and offsets, the values) are copied on s2, and
-// `late` is recorded on s2 after them.
+// (the values, the other modes' coordinates and offsets) are copied on s2,
+// and the events of `arr` (created by the caller) are recorded on s2 as they
+// land.
 int upload_hicoo(ptiB200Tensor *t, const ptiSparseTensorHiCOO *H, cudaStream_t s, int first_mode = -1,
-                 cudaStream_t s2 = nullptr, cudaEvent_t late = nullptr);
+                 cudaStream_t s2 = nullptr, Arrivals *arr = nullptr);
 
 // MTTKRP launchers; factors are device pointers (element type ft), out is FP32.
 // vals_override (optional): nnz values in the tensor's input order that replace
 // its own values (COO tensors only).
-// late (optional): an event after which all of the tensor's arrays are on
-// the device; the schedule build and the kernel wait for it only where they
-// need the arrays it covers.
+// arr (optional): arrival events of the tensor's arrays and the factors; the
+// schedule build and the kernel wait for each only where they read it.
 int mttkrp_device(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t R, uint32_t stride,
                   const uint32_t *mats_order, uint32_t mode, float *out, cudaStream_t s,
-                  const float *vals_override = nullptr, cudaEvent_t late = nullptr);
-int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, cudaEvent_t late = nullptr);
+                  const float *vals_override = nullptr, const Arrivals *arr = nullptr);
+int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals *arr = nullptr);
 
 // Host-struct MTTKRP used by the reference entry points.
 int mttkrp_host_coo(const ptiSparseTensor *X, ptiMatrix **mats, const ptiIndex *mats_order,
