@@ -210,6 +210,19 @@ struct RunWriter {
     }
 };
 
+// True when every record of the batch, in every group of the warp still
+// walking, continues its group's current output row: the batch then needs no
+// row bookkeeping (what RunWriter::start would do for each record is nothing).
+// Deciding for the whole warp keeps its groups on one path.
+template <int U>
+__device__ __forceinline__ bool same_row_batch(const uint32_t (&orow)[U], uint32_t cur)
+{
+    bool same = cur != kNoRow;
+#pragma unroll
+    for (int u = 0; u < U; ++u) same = same && orow[u] == cur;
+    return __all_sync(__activemask(), same);
+}
+
 // Walks records [j0, j1) (ordered by output row) of a tile whose records are
 // s_rec[0, n): gathers the operand rows and accumulates v * prod_k A_k[row_k]
 // in registers, one output row run at a time (RunWriter).
@@ -258,6 +271,13 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
                         f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)wd[1 + k] * a.stride, col);
                 }
             }
+        }
+        if (same_row_batch<U>(orow, w.cur)) {  // no row bookkeeping
+            if (active) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(w.acc, f[u], val[u]);
+            }
+            continue;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -449,6 +469,13 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
                     for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + rr[k], 0);
                 }
             }
+        }
+        if (same_row_batch<U>(orow, w.cur)) {  // no row bookkeeping
+            if (active) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
+            }
+            continue;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
