@@ -316,6 +316,30 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
                 f1[u].load(mat1 + (size_t)s_r1[z] * stride, col);
             }
         }
+        auto add = [&](int u) {
+            const float2 vv = make_float2(v[u], v[u]);
+#pragma unroll
+            for (int c = 0; c < CPL; c += 2) {
+                float2 p;
+                if constexpr (sizeof(FT) == 2) p = bf16x2_mul(f0[u].w[c >> 1], f1[u].w[c >> 1]);
+                else p = __fmul2_rn(make_float2(f0[u].at(c), f0[u].at(c + 1)), make_float2(f1[u].at(c), f1[u].at(c + 1)));
+                const float2 r = __ffma2_rn(p, vv, make_float2(acc[c], acc[c + 1]));
+                acc[c] = r.x;
+                acc[c + 1] = r.y;
+            }
+        };
+        // every group of the warp still walking continues its row: no row
+        // bookkeeping for this batch
+        bool same = cur != 0xFFFFFFFFu;
+#pragma unroll
+        for (int u = 0; u < U; ++u) same = same && orow[u] == cur;
+        if (__all_sync(__activemask(), same)) {
+            if (active) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) add(u);
+            }
+            continue;
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (orow[u] == 0xFFFFFFFFu) continue;
@@ -325,18 +349,7 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
                 for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
                 cur = orow[u];
             }
-            if (active) {
-                const float2 vv = make_float2(v[u], v[u]);
-#pragma unroll
-                for (int c = 0; c < CPL; c += 2) {
-                    float2 p;
-                    if constexpr (sizeof(FT) == 2) p = bf16x2_mul(f0[u].w[c >> 1], f1[u].w[c >> 1]);
-                    else p = __fmul2_rn(make_float2(f0[u].at(c), f0[u].at(c + 1)), make_float2(f1[u].at(c), f1[u].at(c + 1)));
-                    const float2 r = __ffma2_rn(p, vv, make_float2(acc[c], acc[c + 1]));
-                    acc[c] = r.x;
-                    acc[c + 1] = r.y;
-                }
-            }
+            if (active) add(u);
         }
     }
     if (cur != 0xFFFFFFFFu && active) flush(cur);
