@@ -21,6 +21,8 @@
 // into global memory once per run of equal rows (16-byte vector atomics); a
 // row shared by neighbouring groups is merged in shared memory first, so a hot
 // row costs one global add per tile instead of one per nonzero.
+#include <type_traits>
+
 #include "kutil.cuh"
 #include "primitives.cuh"
 #include "tensor.cuh"
@@ -452,14 +454,17 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
     const FT *base[NIN];  // this lane's columns of each operand factor
 #pragma unroll
     for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + col;
-    for (uint32_t j = j0; j < j1; j += U) {
+    // full batches of U records without per-record bounds tests, then one
+    // partial batch
+    auto batch = [&](uint32_t j, auto check) {
+        constexpr bool CHECK = decltype(check)::value;
         uint32_t orow[U];
         float v[U];
         RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             orow[u] = kNoRow;
-            if (j + u < j1) {
+            if (!CHECK || j + u < j1) {
                 const uint4 r = s_rec[j + u];
                 const uint32_t rr[3] = {r.y, r.z, r.w};
                 orow[u] = r.x;
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 #pragma unroll
                 for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
             }
-            continue;
+            return;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -483,7 +488,10 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
             w.start(orow[u], a);
             if (active) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
         }
-    }
+    };
+    uint32_t j = j0;
+    for (; j + U <= j1; j += U) batch(j, std::false_type{});
+    if (j < j1) batch(j, std::true_type{});
     const bool owner = w.finish(a);
     __syncthreads();
     if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
