@@ -433,6 +433,21 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
                   PTIERR_VALUE_ERROR, mod, "checkpoint is of another tensor (sum of squared values differs)");
     }
 
+    // W of a mode needs only the other modes' Grams, so it is computed on a
+    // side stream while that mode's MTTKRP runs on s (fork at ev.g, join at
+    // ev.w before the row solve)
+    struct ForkEvents {
+        cudaEvent_t g = nullptr, w = nullptr;
+        ~ForkEvents()
+        {
+            if (g) cudaEventDestroy(g);
+            if (w) cudaEventDestroy(w);
+        }
+    } ev;
+    PTI_CUDA(cudaEventCreateWithFlags(&ev.g, cudaEventDisableTiming), mod);
+    PTI_CUDA(cudaEventCreateWithFlags(&ev.w, cudaEventDisableTiming), mod);
+    const cudaStream_t side = side_stream(1);
+
     std::vector<uint32_t> order(N);
     std::vector<const void *> fptr(N);
     res.fits.clear();
@@ -446,13 +461,18 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
             fptr[k] = use_bf16 ? (const void *)Ab[k].ptr : (const void *)A[k];
         for (uint32_t m = 0; m < N; ++m) {
             for (uint32_t i = 0; i < N; ++i) order[i] = (m + i) % N;
+            PTI_CUDA(cudaEventRecord(ev.g, s), mod);
+            PTI_CUDA(cudaStreamWaitEvent(side, ev.g, 0), mod);
+            if (R <= 32)
+                gram_inverse_small_kernel<<<1, 256, 0, side>>>(G.as<double>(), N, R, m, W.as<double>(), flag);
+            else
+                gram_inverse_kernel<<<1, 256, 0, side>>>(G.as<double>(), N, R, m, W.as<double>(), work.as<double>(),
+                                                         flag);
+            PTI_CUDA(cudaGetLastError(), mod);
+            PTI_CUDA(cudaEventRecord(ev.w, side), mod);
             PTI_TRY(mttkrp_device(t, fptr.data(), use_bf16 ? PTI_B200_BF16 : PTI_B200_F32, R, stride, order.data(), m,
                                   M.as<float>(), s));
-            if (R <= 32)
-                gram_inverse_small_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), flag);
-            else
-                gram_inverse_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, m, W.as<double>(), work.as<double>(),
-                                                      flag);
+            PTI_CUDA(cudaStreamWaitEvent(s, ev.w, 0), mod);
             PTI_CUDA(cudaMemsetAsync(stats.ptr, 0, (size_t)R * 12, s), mod);
             solve_rows_kernel<<<rows_grid((uint64_t)t->ndims[m] * stride, 256), 256, solve_smem, s>>>(
                 M.as<float>(), W.as<double>(), t->ndims[m], R, stride, A[m], colsq, colmax);
