@@ -251,14 +251,20 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
         s_slot_whole[g] = 0;
     }
     RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
-    for (uint32_t j = j0; j < j1; j += U) {
+    const FT *base[NIN];  // this lane's columns of each operand factor
+#pragma unroll
+    for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + col;
+    // full batches of U records without per-record bounds tests, then one
+    // partial batch
+    auto batch = [&](uint32_t j, auto check) {
+        constexpr bool CHECK = decltype(check)::value;
         uint32_t orow[U];
         float val[U];
         RowPart<CPL, FT> f[U][NIN];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             orow[u] = kNoRow;
-            if (j + u < j1) {
+            if (!CHECK || j + u < j1) {
                 uint32_t wd[RW];
 #pragma unroll
                 for (int q = 0; q < RW; q += 4) {
@@ -269,8 +275,7 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
                 val[u] = alt ? __ldg(alt + j + u) : __uint_as_float(wd[1 + NIN]);
                 if (orow[u] != kNoRow && active) {
 #pragma unroll
-                    for (int k = 0; k < NIN; ++k)
-                        f[u][k].load(static_cast<const FT *>(a.in_mat[k]) + (size_t)wd[1 + k] * a.stride, col);
+                    for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + (size_t)wd[1 + k] * a.stride, 0);
                 }
             }
         }
@@ -279,7 +284,7 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
 #pragma unroll
                 for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(w.acc, f[u], val[u]);
             }
-            continue;
+            return;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -287,7 +292,10 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
             w.start(orow[u], a);
             if (active) accumulate<CPL, FT, NIN>(w.acc, f[u], val[u]);
         }
-    }
+    };
+    uint32_t j = j0;
+    for (; j + U <= j1; j += U) batch(j, std::false_type{});
+    if (j < j1) batch(j, std::true_type{});
     const bool owner = w.finish(a);
     __syncthreads();
     if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
