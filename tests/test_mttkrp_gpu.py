@@ -232,3 +232,38 @@ def test_lock_variant_and_mutex_pool(lib, cuda, orc):
         want = orc.mttkrp_coo(inds, vals, mats, R, mode)[: dims[mode]]
         assert rel_err(out[:, :R], want[:, :R]) < 1e-5
     lib.ptiMutexFree(pool)
+
+
+def _hicoo_by_hand(dims, inds, vals, sb):
+    """A HiCOO tensor of any order built directly: nonzeros sorted by block
+    coordinates (lexicographically), one block per distinct tuple."""
+    N = len(dims)
+    bl = [(i >> sb).astype(np.int64) for i in inds]
+    order = np.lexsort(tuple(bl[::-1]))
+    bl = [b[order] for b in bl]
+    change = np.ones(vals.size, bool)
+    change[1:] = np.any([b[1:] != b[:-1] for b in bl], axis=0)
+    starts = np.flatnonzero(change)
+    bptr = np.append(starts, vals.size).astype(np.uint64)
+    binds = [b[starts].astype(np.uint32) for b in bl]
+    einds = [(inds[m][order] & ((1 << sb) - 1)).astype(np.uint8) for m in range(N)]
+    return bptr, binds, einds, vals[order].copy()
+
+
+@pytest.mark.parametrize("N", [2, 5])
+def test_hicoo_dropin_other_orders(lib, cuda, orc, N):
+    """ptiMTTKRPHiCOO on hand-built 2-D and 5-D HiCOO tensors (the reference's
+    conversion makes only 3-D and 4-D ones): the copies of the arrays a mode's
+    schedule does not start from overlap the schedule build, and the result
+    must still equal the oracle's COO MTTKRP."""
+    dims = (300, 200) if N == 2 else (12, 10, 9, 8, 7)
+    nnz = 20000 if N == 2 else 15000
+    inds, vals = synth.uniform_tensor(dims, nnz, seed=N + 50)
+    R = 16
+    mats = synth.factor_matrices(dims, R, seed=N + 51)
+    sb = 3 if N == 2 else 2
+    bptr, binds, einds, hv = _hicoo_by_hand(dims, inds, vals, sb)
+    ht = HiCOOTensor(dims, sb, sb + 2, sb + 3, bptr, binds, einds, hv)
+    for m in range(N):
+        ref = orc.mttkrp_coo(inds, vals, mats, R, m)[: dims[m]]
+        _check(ht.mttkrp(mats, R, m), ref)
