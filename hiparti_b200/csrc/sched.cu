@@ -52,6 +52,7 @@ struct SchedArgs {
     const float *vals;
     float *out;
     uint32_t *err;
+    const uint4 *bquad;         // HiCOO 4-D: per block {output, operand 0, 1, 2} block coordinates
 };
 
 
@@ -366,18 +367,27 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
         mbar_fence_init();
     }
     __syncthreads();
+    // 4-D: the blocks' four coordinates come as one 16-byte record each, so a
+    // nonzero's decode reads them with one shared-memory load
+    const uint4 *s_bq = reinterpret_cast<const uint4 *>(sm + L::brow);
     if (tid == 0) {
         const uint32_t be = round16(n), bv = round16(4 * n), bl = round16(2 * n);
         const uint32_t bb = 4 * ((nblk + bo4 + 3) & ~3u);
-        mbar_arrive_expect_tx(&mbar, bv + (NIN + 1) * be + bl + (NIN + 1) * bb);
+        const uint32_t bq = 16 * nblk;
+        mbar_arrive_expect_tx(&mbar, bv + (NIN + 1) * be + bl + (NIN == 3 ? bq : (NIN + 1) * bb));
         bulk_g2s_ef(s_val, a.vals + z0, bv, &mbar);
         bulk_g2s_ef(s_eout, a.out_eind + z0, be, &mbar);
 #pragma unroll
         for (int k = 0; k < NIN; ++k) bulk_g2s_ef(s_ein + k * kHiTile, a.in_eind[k] + z0, be, &mbar);
         bulk_g2s_ef(s_blk, a.lblk + z0, bl, &mbar);
-        bulk_g2s_ef(s_brow, a.out_bind + (b0 - bo4), bb, &mbar);
+        if constexpr (NIN == 3) {
+            bulk_g2s_ef(sm + L::brow, a.bquad + b0, bq, &mbar);
+        } else {
+            bulk_g2s_ef(s_brow, a.out_bind + (b0 - bo4), bb, &mbar);
 #pragma unroll
-        for (int k = 0; k < NIN; ++k) bulk_g2s_ef(s_bin + k * (kHiTile + 4), a.in_bind[k] + (b0 - bo4), bb, &mbar);
+            for (int k = 0; k < NIN; ++k)
+                bulk_g2s_ef(s_bin + k * (kHiTile + 4), a.in_bind[k] + (b0 - bo4), bb, &mbar);
+        }
     }
     const bool ok = mbar_wait_bounded(&mbar, 0);
     if (!__syncthreads_and(ok)) {
@@ -404,12 +414,24 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
             vv[p] = 0.f;
             if (z < n) {
                 const uint32_t i = s_blk[z];
-                const uint32_t o = (s_brow[i] << a.sb) + s_eout[z];
+                uint32_t bo, bi[3];
+                if constexpr (NIN == 3) {
+                    const uint4 q = s_bq[i < nblk ? i : 0];
+                    bo = q.x;
+                    bi[0] = q.y;
+                    bi[1] = q.z;
+                    bi[2] = q.w;
+                } else {
+                    bo = s_brow[i];
+#pragma unroll
+                    for (int k = 0; k < NIN; ++k) bi[k] = s_bin[k * (kHiTile + 4) + i];
+                }
+                const uint32_t o = (bo << a.sb) + s_eout[z];
                 uint32_t r[3] = {0u, 0u, 0u};
                 bool ok_z = i < nblk && o < a.out_dim;
 #pragma unroll
                 for (int k = 0; k < NIN; ++k) {
-                    r[k] = (s_bin[k * (kHiTile + 4) + i] << a.sb) + s_ein[k * kHiTile + z];
+                    r[k] = (bi[k] << a.sb) + s_ein[k * kHiTile + z];
                     ok_z = ok_z && r[k] < a.in_dim[k];
                 }
                 vv[p] = s_val[z];
@@ -554,6 +576,15 @@ __global__ void iota_keys_kernel(const uint32_t *src, uint64_t n, uint64_t *keys
         keys[i] = src[i];
         vals[i] = (uint32_t)i;
     }
+}
+
+// 4-D schedules: each block's coordinates as one record {output mode,
+// operand modes in increasing order}.
+__global__ void pack_bquad_kernel(const uint32_t *bo, const uint32_t *b0, const uint32_t *b1, const uint32_t *b2,
+                                  uint64_t nb, uint4 *q)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (uint64_t)gridDim.x * blockDim.x)
+        q[i] = make_uint4(bo[i], b0[i], b1[i], b2[i]);
 }
 
 // COO packed records in sorted order: {out index, operand indices (modes in
@@ -802,6 +833,15 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals
         for (uint32_t k = 0; k < N; ++k)
             if (k != mode) PTI_TRY(gather_mode(k));
         bperm.reset();
+        if (N == 4) {
+            uint32_t o[3], c = 0;
+            for (uint32_t k = 0; k < N; ++k)
+                if (k != mode) o[c++] = k;
+            PTI_CUDA(P.bquad.alloc(padded(nb * 16), s), mod);
+            pack_bquad_kernel<<<grid_n(nb), 256, 0, s>>>(P.binds[mode].as<uint32_t>(), P.binds[o[0]].as<uint32_t>(),
+                                                         P.binds[o[1]].as<uint32_t>(), P.binds[o[2]].as<uint32_t>(),
+                                                         nb, P.bquad.as<uint4>());
+        }
     }
     inv.reset();
     PTI_CUDA(cudaGetLastError(), mod);
@@ -922,13 +962,20 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
         a.tile_block = P.tile_block.as<uint32_t>();
         a.out_bind = P.binds[mode].as<uint32_t>();
         a.out_eind = P.einds[mode].as<uint8_t>();
-        for (uint32_t i = 1; i < N; ++i) {
-            const uint32_t k = mats_order[i];
+        // 4-D: the operands in increasing mode order, the order of the block
+        // records (the product's order only changes FP32 rounding)
+        for (uint32_t i = 1, c = 0; i < N; ++i) {
+            uint32_t k = mats_order[i];
+            if (N == 4) {
+                while (c == mode) ++c;
+                k = c++;
+            }
             a.in_bind[i - 1] = P.binds[k].as<uint32_t>();
             a.in_eind[i - 1] = P.einds[k].as<uint8_t>();
             a.in_dim[i - 1] = t->ndims[k];
             a.in_mat[i - 1] = mats[k];
         }
+        a.bquad = N == 4 ? P.bquad.as<uint4>() : nullptr;
         a.vals = P.vals.as<float>();
     } else {
         // records hold the operand modes in increasing order

@@ -30,6 +30,7 @@ struct HicooModePlan {
     DevBuf lblk;                          // uint16 [nnz]: block of the nonzero - tile_block[tile]
     DevBuf tile_block;                    // uint32 [ntiles+1]: first block of each tile
     uint32_t ntiles = 0;
+    DevBuf bquad;                         // 4-D: uint4 [nb], {output, operands in increasing mode order}
 };
 
 // Per-mode schedule of a COO tensor: nonzeros sorted by the output-mode index,
