@@ -16,7 +16,7 @@ the workload (the path does not shard; no collective), value = all ranks'
 bytes / max time.
 
 --impl reference times the reference's own OpenMP CPU code (oracle/_ref,
-compiled from the reference sources) on a bounded sample of the workload.
+compiled from the reference sources) on the same 50M-nonzero tensor.
 """
 from __future__ import annotations
 
@@ -884,13 +884,91 @@ def download_hicoo(h):
     return {"bptr": bptr, "binds": binds, "einds": einds, "vals": vals}
 
 
+def c2_host_tensor(seed=SEED, nnz=C2_NNZ):
+    """The C2 tensor and factors exactly as run_ours_mttkrp builds them (same
+    generator, same seeds), brought to host memory.  Generation runs on the
+    GPU with torch when one is present (de-duplicating 65M coordinates takes
+    milliseconds there and minutes with numpy); this is data generation only,
+    outside every timed region."""
+    import torch
+    from hiparti_b200.synth import coords_torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ti = coords_torch(C2_DIMS, nnz, seed, zipf_s=1.1, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    tv = torch.rand(nnz, generator=g, device=dev, dtype=torch.float32)
+    inds = [t.cpu().numpy().view(np.uint32) for t in ti]
+    vals = tv.cpu().numpy()
+    mats = [m.cpu().numpy() for m in c2_factors(dev, seed)]
+    del ti, tv
+    torch.cuda.empty_cache()
+    return inds, vals, mats
+
+
 def run_reference_arm(args, rank, world):
     """Times the reference's own CPU code (oracle/_ref/libHiParTI.so, built
-    from its sources): ptiSparseTensorToHiCOO (tk=1, untimed) on a sample of
-    the C2 tensor, then ptiOmpMTTKRPHiCOO with every host thread, 3 modes per
-    step."""
+    from its sources) on the benchmark workload itself: the 50M-nonzero C2
+    tensor of run_ours_mttkrp (same seeds), converted by the reference's
+    ptiSparseTensorToHiCOO(tk=1) (untimed, as the reference's driver
+    benchmark/tensor/mttkrp_hicoo.c converts before its timed loop), then
+    ptiOmpMTTKRPHiCOO with every host thread, 3 modes per step.  Under torchrun
+    rank 0 alone runs; the other ranks return without work."""
     if rank != 0:
         return None
+    from oracle.oracle import Ref, ensure_built
+    try:
+        ensure_built(ref=True)
+    except Exception:
+        pass
+    if not Ref.available():
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref not built (needs its sources)"}
+    import torch
+    if not torch.cuda.is_available():
+        return {"impl": "reference", "unavailable": "the C2 tensor is generated on a CUDA device; none present"}
+    ref = Ref()
+    threads = os.cpu_count() or 1
+    nnz = args.nnz
+    t0 = time.perf_counter()
+    inds, vals, mats = c2_host_tensor(SEED, nnz)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    h = ref.to_hicoo(list(C2_DIMS), inds, vals, C2_SB, C2_SK, C2_SC)
+    conv_s = time.perf_counter() - t0
+    del inds, vals
+    nb = h["bptr"].size - 1
+    run = ref.omp_hicoo_mttkrp_runner(list(C2_DIMS), h, mats, C2_R, threads)
+    N = 3
+    for _ in range(args.warmup):
+        for m in range(N):
+            run(m)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for m in range(N):
+            run(m)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    step_bytes = N * hicoo_bytes(nnz, nb, C2_DIMS, C2_R, N)
+    value = step_bytes / dt / 1e9
+    sample_desc = (f"the full workload: {nnz} unique nonzeros of the C2 construction (seed {SEED}, the tensor "
+                   f"--impl ours times), nb={nb}; HiCOO built by the reference's ptiSparseTensorToHiCOO(tk=1) "
+                   f"in {conv_s:.1f} s, untimed; one step = ptiOmpMTTKRPHiCOO(tk={threads}, tb=1) for modes 0,1,2")
+    return {"metric": "hicoo_mttkrp_GBps", "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Zipf(1.1) coordinates, U(0,1) values and factors)", "impl": "reference",
+            "config": {"workload": f"C2 HiCOO MTTKRP, 3-D 200000x150000x20000, {nnz // 1000000}M nnz Zipf(1.1), "
+                                   "R=32, sb=7 sk=10 sc=14, FP32, all 3 modes per step",
+                       "nnz": nnz, "nb": nb, "rank": C2_R, "modes_per_step": N,
+                       "algorithmic_bytes_per_step": step_bytes, "generation_s": round(gen_s, 1),
+                       "reference_conversion_s": round(conv_s, 2), "parallelism": "reference OpenMP, rank 0"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+                             "sample": sample_desc},
+            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_sample(args):
+    """cpu_baseline of our own line: the reference's ptiOmpMTTKRPHiCOO on a
+    bounded sample of the C2 construction (rank 0, N = 1), so that the default
+    run stays within minutes; the full-size reference run is --impl reference."""
     from oracle.oracle import Ref, ensure_built
     from hiparti_b200.synth import coords_numpy
     try:
@@ -898,7 +976,8 @@ def run_reference_arm(args, rank, world):
     except Exception:
         pass
     if not Ref.available():
-        return {"impl": "reference", "unavailable": "reference library oracle/_ref not built (needs its sources)"}
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference library oracle/_ref not built (needs its sources)"}
     ref = Ref()
     threads = os.cpu_count() or 1
     sample = args.ref_sample
@@ -909,29 +988,19 @@ def run_reference_arm(args, rank, world):
     rng = np.random.default_rng(SEED + 2)
     stride = ((C2_R - 1) // 8 + 1) * 8
     mats = [rng.random((d, stride), dtype=np.float32) for d in C2_DIMS]
+    run = ref.omp_hicoo_mttkrp_runner(list(C2_DIMS), h, mats, C2_R, threads)
     N = 3
-    for _ in range(args.warmup):
-        for m in range(N):
-            ref.mttkrp_hicoo(list(C2_DIMS), h, mats, C2_R, m, variant="omp", tk=threads)
+    for m in range(N):
+        run(m)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for m in range(N):
-            ref.mttkrp_hicoo(list(C2_DIMS), h, mats, C2_R, m, variant="omp", tk=threads)
-    dt = (time.perf_counter() - t0) / args.steps
-    step_bytes = N * hicoo_bytes(sample, nb, C2_DIMS, C2_R, N)
-    value = step_bytes / dt / 1e9
-    sample_desc = (f"{sample} unique nonzeros drawn by the C2 construction (same dims, Zipf(1.1) per mode, "
-                   f"U(0,1) values), nb={nb}; HiCOO built by the reference's ptiSparseTensorToHiCOO(tk=1), "
-                   f"untimed; one step = ptiOmpMTTKRPHiCOO(tk={threads}, tb=1) for modes 0,1,2")
-    return {"metric": "hicoo_mttkrp_GBps", "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": "C2 HiCOO MTTKRP sample (reference ptiOmpMTTKRPHiCOO, tk=all host threads)",
-                       "nnz": sample, "nb": nb, "rank": C2_R},
-            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
-                             "sample": sample_desc},
-            "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    for m in range(N):
+        run(m)
+    dt = time.perf_counter() - t0
+    value = N * hicoo_bytes(sample, nb, C2_DIMS, C2_R, N) / dt / 1e9
+    return {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+            "sample": (f"{sample} unique nonzeros drawn by the C2 construction (same dims, Zipf(1.1) per mode, "
+                       f"U(0,1) values), nb={nb}; HiCOO built by the reference's ptiSparseTensorToHiCOO(tk=1), "
+                       f"untimed; one step = ptiOmpMTTKRPHiCOO(tk={threads}, tb=1) for modes 0,1,2")}
 
 
 C1_DIMS = (1000, 1000, 1000)
@@ -1049,11 +1118,7 @@ def run_cpu_paths(args):
 
 def cpu_baseline_block(args):
     """Reference OpenMP HiCOO MTTKRP on a bounded sample (rank 0, N=1)."""
-    res = run_reference_arm(argparse.Namespace(warmup=0, steps=1, ref_sample=args.ref_sample), 0, 1)
-    if res is None or "unavailable" in res:
-        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": res.get("unavailable") if res else "n/a"}
-    return res["cpu_baseline"]
+    return run_reference_sample(args)
 
 
 def main():

@@ -207,9 +207,10 @@ __device__ __forceinline__ uint32_t round16u(uint32_t x) { return (x + 15u) & ~1
 // nonzero (the group size is chosen from the tensor's rank at run time, so a
 // kernel holds one tile variant).  The schedule keeps each tile's nonzeros in
 // output-row order, so a group walks a contiguous slice and adds a row into
-// M once per run.
+// M once per run.  Returns false (uniformly over the CTA) if the tile's bulk
+// copies did not complete within the wait bound.
 template <int CPL, class FT>
-__device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsigned char *sm, uint64_t *mbar,
+__device__ bool tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsigned char *sm, uint64_t *mbar,
                           uint32_t &phase, uint32_t *err)
 {
     constexpr int U = 4;  // nonzeros in flight per group
@@ -246,11 +247,18 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
         bulk_g2s_ef(s_bin + (kBTile + 4), gp->in_bind[1] + (b0 - bo4), bb, mbar);
     }
     const bool ok = mbar_wait_bounded(mbar, phase);
-    phase ^= 1u;
     if (!__syncthreads_and(ok)) {
-        if (tid == 0) atomicOr(err, kErrCopy);
-        return;
+        // Copies still in flight would land in the staging area of a later
+        // task: wait once more (bounded) for this phase.  The caller then
+        // stops issuing bulk copies in this CTA, so the barrier is never
+        // re-armed while this phase may still be open.
+        if (tid == 0) {
+            atomicOr(err, kErrCopy);
+            mbar_wait_bounded(mbar, phase);
+        }
+        return false;
     }
+    phase ^= 1u;
     s_brow += bo4;
     s_bin += bo4;
     // decode every nonzero once: output row (or a marker for a bad
@@ -353,6 +361,7 @@ __device__ void tile_task(const BatchPlan *__restrict__ gp, uint32_t tile, unsig
         }
     }
     if (cur != 0xFFFFFFFFu && active) flush(cur);
+    return true;
 }
 
 // Block-wide sum of one double per thread; the result is returned to every
@@ -621,6 +630,7 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
         mbar_fence_init();
     }
     uint32_t phase = 0;
+    bool copies_ok = true;  // false once a tile's bulk copies missed their wait bound
     __syncthreads();
     for (;;) {
         if (tid == 0) s_q = atomicAdd(head, 1u);
@@ -640,7 +650,7 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
         __syncthreads();
         if (s_ok) {
             if (dense) dense_task(a.tens + b, b, m, it, a, sm);
-            else tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err);
+            else if (copies_ok) copies_ok = tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err);
         }
         // shared memory written by this task may next be filled by bulk copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -20,6 +20,10 @@
 // ssyrk_ call does not write, so its printed fit is not the model's fit.)
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
 #include "checkpoint.cuh"
 #include "spd.cuh"
 #include "tensor.cuh"
@@ -335,6 +339,7 @@ struct CpdOptions {
     const char *ckpt_path = nullptr;  // checkpoint file (nullptr: none)
     uint32_t ckpt_every = 0;          // write after every ckpt_every iterations; always after the last
     bool resume = false;              // continue from ckpt_path when the file exists
+    float *m_last = nullptr;          // device, ndims[N-1] x stride: receives the last MTTKRP output
 };
 
 struct CpdResult {
@@ -502,6 +507,9 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
             PTI_TRY(writer.save(A, stride, lambda, fits, normX2, it + 1, converged, s));
     }
     res.iters = it;
+    if (opt.m_last && it > 0 && t->ndims[N - 1])
+        PTI_CUDA(cudaMemcpyAsync(opt.m_last, M.ptr, (size_t)t->ndims[N - 1] * stride * 4, cudaMemcpyDeviceToDevice, s),
+                 mod);
     // GetFinalLambda (matrix.c:556-572)
     for (uint32_t m = 0; m < N; ++m) {
         PTI_CUDA(cudaMemsetAsync(colsq, 0, (size_t)R * 8, s), mod);
@@ -626,6 +634,468 @@ int cpd_hicoo_entry(const ptiSparseTensorHiCOO *H, ptiIndex R, ptiIndex niters, 
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// The reference's dense ALS helpers and its ALS step with caller-seeded
+// factors, as GPU calls on host matrices.  Each copies its operands to the
+// device, runs there and copies the results back (the calls are small; a
+// caller that keeps everything on the device uses ptiB200CpdAls).
+// ---------------------------------------------------------------------------
+
+// Grams as the reference keeps them: R x stride FP32, only the row-major
+// upper triangle (i <= j) guaranteed written -- the part its ssyrk_('L') calls
+// fill (src/sptensor/cpd.c:68,128).  out32 = the FP32 product of `count`
+// Grams in the given order, mirrored to a full symmetric matrix
+// (src/matrix/matrix.c:340-385); out64 = the same product in FP64 (R x R).
+__global__ void tri_hadamard_kernel(const float *grams, uint32_t count, uint32_t R, uint32_t stride, float *out32,
+                                    double *out64)
+{
+    for (uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+        const uint32_t i = e / R, j = e % R;
+        const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+        float v = 1.f;
+        double w = 1.0;
+        for (uint32_t k = 0; k < count; ++k) {
+            const float gk = grams[(size_t)k * R * stride + (size_t)lo * stride + hi];
+            v *= gk;
+            w *= (double)gk;
+        }
+        if (out32) out32[(size_t)i * stride + j] = v;
+        if (out64) out64[e] = w;
+    }
+}
+
+// FP64 column statistics of a matrix: sums of squares and the largest
+// positive entry (int bits of the FP32 value; 0 when there is none).
+__global__ void colstat_kernel(const float *A, uint32_t I, uint32_t R, uint32_t stride, double *colsq, int *colmax)
+{
+    extern __shared__ double s_sq[];
+    int *s_mx = reinterpret_cast<int *>(s_sq + R);
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        s_sq[c] = 0.0;
+        s_mx[c] = 0;
+    }
+    __syncthreads();
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c >= R) continue;
+        const float v = A[e];
+        atomicAdd(&s_sq[c], (double)v * (double)v);
+        if (v > 0.f) atomicMax(&s_mx[c], __float_as_int(v));
+    }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        atomicAdd(&colsq[c], s_sq[c]);
+        atomicMax(&colmax[c], s_mx[c]);
+    }
+}
+
+// A[:, c] /= lambda[c] for the first R columns (pad columns untouched).
+__global__ void div_cols_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, const float *lambda)
+{
+    const uint64_t total = (uint64_t)I * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e % stride);
+        if (c < R) A[e] = A[e] / lambda[c];
+    }
+}
+
+// |lambda^T (Hadamard_m G_m) lambda| over N Grams read from their row-major
+// upper triangles (FP64), and the FP32 Hadamard product, full symmetric, into
+// prod (the reference's scratch ata[nmodes], src/ktensor/ktensor.c:105-147).
+__global__ void kruskal_normsq_kernel(const float *grams, uint32_t N, uint32_t R, uint32_t stride, const float *lambda,
+                                      float *prod, double *out)
+{
+    __shared__ double s_part[32];
+    double s = 0.0;
+    for (uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+        const uint32_t i = e / R, j = e % R;
+        const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+        float v = 1.f;
+        double w = 1.0;
+        for (uint32_t k = 0; k < N; ++k) {
+            const float gk = grams[(size_t)k * R * stride + (size_t)lo * stride + hi];
+            v *= gk;
+            w *= (double)gk;
+        }
+        if (prod) prod[(size_t)i * stride + j] = v;
+        s += w * (double)lambda[i] * (double)lambda[j];
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) t += s_part[w];
+        out[0] = fabs(t);
+    }
+}
+
+namespace {
+
+unsigned rows_grid_for(uint64_t items)
+{
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + 255) / 256, (uint64_t)sm_count() * 4));
+}
+
+// Device copy of the first `rows` rows (stride floats each) of host matrices,
+// laid out one after another.
+template <class Mat>
+int upload_mats(DevBuf &buf, Mat *const *mats, const uint32_t *which, uint32_t count, uint32_t rows,
+                uint32_t stride, cudaStream_t s, const char *mod)
+{
+    const size_t one = (size_t)rows * stride;
+    PTI_CUDA(buf.alloc(padded(std::max<size_t>(1, count * one) * 4), s), mod);
+    for (uint32_t k = 0; k < count; ++k)
+        if (one)
+            PTI_CUDA(cudaMemcpyAsync(buf.as<float>() + k * one, mats[which ? which[k] : k]->values, one * 4,
+                                     cudaMemcpyHostToDevice, s),
+                     mod);
+    return 0;
+}
+
+// Grams aTa[0..nmodes] (R x R, one stride): same rank, stride and row count,
+// as the reference asserts (src/matrix/matrix.c:345-348).
+template <class Mat>
+int check_grams(uint32_t nmodes, Mat **aTa, uint32_t upto, const char *mod)
+{
+    PTI_CHECK(aTa && nmodes >= 1, PTIERR_VALUE_ERROR, mod, "null matrices");
+    for (uint32_t m = 0; m <= upto; ++m) PTI_CHECK(aTa[m] && aTa[m]->values, PTIERR_VALUE_ERROR, mod, "null matrix");
+    const uint32_t R = aTa[0]->ncols, st = aTa[0]->stride;
+    PTI_CHECK(R >= 1 && st >= R && aTa[0]->nrows >= R, PTIERR_SHAPE_MISMATCH, mod, "Gram must be rank x rank");
+    for (uint32_t m = 1; m <= upto; ++m)
+        PTI_CHECK((uint32_t)aTa[m]->ncols == R && (uint32_t)aTa[m]->stride == st && aTa[m]->nrows == aTa[0]->nrows,
+                  PTIERR_SHAPE_MISMATCH, mod, "Grams differ in shape");
+    return 0;
+}
+
+// ptiMatrixDotMulSeqTriangle, and with rhs the solve of ptiMatrixSolveNormals
+// (src/matrix/matrix_solver.c:32-83): rhs <- rhs (Hadamard_{k != mode} aTa_k)^{-1}.
+// aTa[nmodes] receives the FP32 Hadamard product, full symmetric.  The solve
+// factors the FP64 product of the same Grams (Cholesky; Gauss-Jordan if it is
+// not positive definite, as the reference falls back to sgesv; a singular
+// matrix leaves rhs unchanged, as a failed sgesv does).
+template <class Mat>
+int normals(uint32_t mode, uint32_t nmodes, Mat **aTa, Mat *rhs, const char *mod)
+{
+    PTI_TRY(check_grams(nmodes, aTa, nmodes, mod));
+    PTI_CHECK(mode < nmodes, PTIERR_VALUE_ERROR, mod, "mode out of range");
+    const uint32_t R = aTa[0]->ncols, stride = aTa[0]->stride;
+    if (rhs) {
+        PTI_CHECK(rhs->values || rhs->nrows == 0, PTIERR_VALUE_ERROR, mod, "null right-hand side");
+        PTI_CHECK((uint32_t)rhs->ncols == R && (uint32_t)rhs->stride == stride, PTIERR_SHAPE_MISMATCH, mod,
+                  "right-hand side must have the Grams' rank and stride");
+        PTI_CHECK(R <= (uint32_t)kMaxCpdRank, PTIERR_VALUE_ERROR, mod, "rank must be at most 128");
+    }
+    cudaStream_t s = sync_stream();
+    std::vector<uint32_t> order;
+    for (uint32_t m = 1; m < nmodes; ++m) order.push_back((mode + m) % nmodes);
+    DevBuf grams, out32, out64;
+    PTI_TRY(upload_mats(grams, aTa, order.data(), (uint32_t)order.size(), R, stride, s, mod));
+    PTI_TRY(upload_mats(out32, aTa, &nmodes, 1, R, stride, s, mod));
+    if (rhs) PTI_CUDA(out64.alloc(padded((size_t)R * R * 8), s), mod);
+    tri_hadamard_kernel<<<1, 256, 0, s>>>(grams.as<float>(), (uint32_t)order.size(), R, stride, out32.as<float>(),
+                                          rhs ? out64.as<double>() : nullptr);
+    PTI_CUDA(cudaGetLastError(), mod);
+    PTI_CUDA(cudaMemcpyAsync(aTa[nmodes]->values, out32.ptr, (size_t)R * stride * 4, cudaMemcpyDeviceToHost, s), mod);
+    if (rhs && rhs->nrows) {
+        const uint32_t I = rhs->nrows;
+        DevBuf W, work, flag, Min, Aout, stats;
+        PTI_CUDA(W.alloc(padded((size_t)R * R * 8), s), mod);
+        PTI_CUDA(flag.alloc(64, s), mod);
+        // the inverse kernels multiply the Grams of every mode but `mode`; with
+        // the one product matrix as "mode 0 of two", that is the product itself
+        if (R <= 32) {
+            gram_inverse_small_kernel<<<1, 256, 0, s>>>(out64.as<double>(), 2, R, 1, W.as<double>(), flag.as<int>());
+        } else {
+            PTI_CUDA(work.alloc(padded((size_t)3 * R * R * 8), s), mod);
+            gram_inverse_kernel<<<1, 256, 0, s>>>(out64.as<double>(), 2, R, 1, W.as<double>(), work.as<double>(),
+                                                  flag.as<int>());
+        }
+        PTI_CUDA(Min.alloc(padded((size_t)I * stride * 4), s), mod);
+        PTI_CUDA(Aout.alloc(padded((size_t)I * stride * 4), s), mod);
+        PTI_CUDA(stats.alloc(padded((size_t)R * 12 + 64), s), mod);
+        PTI_CUDA(cudaMemsetAsync(stats.ptr, 0, (size_t)R * 12, s), mod);
+        PTI_CUDA(cudaMemcpyAsync(Min.ptr, rhs->values, (size_t)I * stride * 4, cudaMemcpyHostToDevice, s), mod);
+        const size_t solve_smem = (size_t)R * R * 8 + (size_t)R * 12;
+        PTI_CUDA(cudaFuncSetAttribute(solve_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem),
+                 mod);
+        solve_rows_kernel<<<rows_grid_for((uint64_t)I * stride), 256, solve_smem, s>>>(
+            Min.as<float>(), W.as<double>(), I, R, stride, Aout.as<float>(), stats.as<double>(),
+            reinterpret_cast<int *>(stats.as<double>() + R));
+        PTI_CUDA(cudaGetLastError(), mod);
+        int hflag = 0;
+        PTI_CUDA(cudaMemcpyAsync(&hflag, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+        if (hflag != 2)
+            PTI_CUDA(cudaMemcpyAsync(rhs->values, Aout.ptr, (size_t)I * stride * 4, cudaMemcpyDeviceToHost, s), mod);
+    }
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
+// ptiMatrix2Norm (use_2norm) / ptiMatrixMaxNorm (src/matrix/matrix.c:389-553):
+// lambda = column 2-norms, or max(largest entry, 1); columns divided by it.
+template <class Mat>
+int col_normalize(Mat *A, float *lambda, int use_2norm, const char *mod)
+{
+    PTI_CHECK(A && lambda && (A->values || A->nrows == 0), PTIERR_VALUE_ERROR, mod, "null argument");
+    const uint32_t I = A->nrows, R = A->ncols, stride = A->stride;
+    PTI_CHECK(stride >= R, PTIERR_SHAPE_MISMATCH, mod, "stride below ncols");
+    if (R == 0) return 0;
+    cudaStream_t s = sync_stream();
+    DevBuf dA, stats, lam;
+    PTI_CUDA(dA.alloc(padded(std::max<size_t>(1, (size_t)I * stride) * 4), s), mod);
+    PTI_CUDA(stats.alloc(padded((size_t)R * 12 + 64), s), mod);
+    PTI_CUDA(lam.alloc(padded((size_t)R * 4), s), mod);
+    PTI_CUDA(cudaMemsetAsync(stats.ptr, 0, (size_t)R * 12, s), mod);
+    double *colsq = stats.as<double>();
+    int *colmax = reinterpret_cast<int *>(colsq + R);
+    if (I) {
+        PTI_CUDA(cudaMemcpyAsync(dA.ptr, A->values, (size_t)I * stride * 4, cudaMemcpyHostToDevice, s), mod);
+        colstat_kernel<<<rows_grid_for((uint64_t)I * stride), 256, (size_t)R * 12, s>>>(dA.as<float>(), I, R, stride,
+                                                                                       colsq, colmax);
+    }
+    lambda_kernel<<<1, 128, 0, s>>>(colsq, colmax, R, use_2norm, lam.as<float>());
+    if (I) div_cols_kernel<<<rows_grid_for((uint64_t)I * stride), 256, 0, s>>>(dA.as<float>(), I, R, stride,
+                                                                              lam.as<float>());
+    PTI_CUDA(cudaGetLastError(), mod);
+    if (I) PTI_CUDA(cudaMemcpyAsync(A->values, dA.ptr, (size_t)I * stride * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaMemcpyAsync(lambda, lam.ptr, (size_t)R * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
+// GetFinalLambda (src/matrix/matrix.c:556-572): every factor's columns to unit
+// 2-norm, lambda multiplied by the norms.
+template <class Mat>
+int final_lambda(uint32_t rank, uint32_t nmodes, Mat **mats, float *lambda, const char *mod)
+{
+    PTI_CHECK(mats && lambda, PTIERR_VALUE_ERROR, mod, "null argument");
+    cudaStream_t s = sync_stream();
+    DevBuf lam, colsq;
+    PTI_CUDA(lam.alloc(padded((size_t)rank * 4), s), mod);
+    PTI_CUDA(colsq.alloc(padded((size_t)rank * 8), s), mod);
+    PTI_CUDA(cudaMemcpyAsync(lam.ptr, lambda, (size_t)rank * 4, cudaMemcpyHostToDevice, s), mod);
+    for (uint32_t m = 0; m < nmodes; ++m) {
+        Mat *A = mats[m];
+        PTI_CHECK(A && (uint32_t)A->ncols == rank && A->stride >= rank && (A->values || !A->nrows),
+                  PTIERR_SHAPE_MISMATCH, mod, "factor must have `rank` columns");
+        const uint32_t I = A->nrows, stride = A->stride;
+        DevBuf dA;
+        PTI_CUDA(dA.alloc(padded(std::max<size_t>(1, (size_t)I * stride) * 4), s), mod);
+        PTI_CUDA(cudaMemsetAsync(colsq.ptr, 0, (size_t)rank * 8, s), mod);
+        if (I) {
+            PTI_CUDA(cudaMemcpyAsync(dA.ptr, A->values, (size_t)I * stride * 4, cudaMemcpyHostToDevice, s), mod);
+            colsq_kernel<<<rows_grid_for((uint64_t)I * stride), 256, (size_t)rank * 8, s>>>(dA.as<float>(), I, rank,
+                                                                                           stride, colsq.as<double>());
+        }
+        final_scale_kernel<<<rows_grid_for((uint64_t)std::max<uint32_t>(I, 1) * stride), 256, 0, s>>>(
+            dA.as<float>(), I, rank, stride, colsq.as<double>(), lam.as<float>(), 1);
+        PTI_CUDA(cudaGetLastError(), mod);
+        if (I) PTI_CUDA(cudaMemcpyAsync(A->values, dA.ptr, (size_t)I * stride * 4, cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+    }
+    PTI_CUDA(cudaMemcpyAsync(lambda, lam.ptr, (size_t)rank * 4, cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
+// lambda^T (Hadamard_m ata_m) lambda (src/ktensor/ktensor.c:105-147) from the
+// Grams' row-major upper triangles -- the triangle the reference's ssyrk_
+// calls write; its own loop reads the other one.  ata[nmodes] receives the
+// FP32 Hadamard product.  NaN on bad arguments (last error set).
+template <class Mat>
+double kruskal_normsq(uint32_t nmodes, const float *lambda, Mat **ata, const char *mod)
+{
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    if (!lambda || check_grams(nmodes, ata, nmodes, mod) != 0) {
+        if (!lambda) complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "null lambda");
+        return nan;
+    }
+    const uint32_t R = ata[0]->ncols, stride = ata[0]->stride;
+    cudaStream_t s = sync_stream();
+    DevBuf grams, prod, lam, out;
+    double h = nan;
+    if (upload_mats(grams, ata, (const uint32_t *)nullptr, nmodes, R, stride, s, mod) != 0 ||
+        upload_mats(prod, ata, &nmodes, 1, R, stride, s, mod) != 0 || lam.alloc(padded((size_t)R * 4), s) != cudaSuccess ||
+        out.alloc(64, s) != cudaSuccess) {
+        complain(mod, PTIERR_CUDA_ERROR, __FILE__, __LINE__, "device allocation or copy failed");
+        return nan;
+    }
+    cudaMemcpyAsync(lam.ptr, lambda, (size_t)R * 4, cudaMemcpyHostToDevice, s);
+    kruskal_normsq_kernel<<<1, 256, 0, s>>>(grams.as<float>(), nmodes, R, stride, lam.as<float>(), prod.as<float>(),
+                                            out.as<double>());
+    cudaMemcpyAsync(ata[nmodes]->values, prod.ptr, (size_t)R * stride * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h, out.ptr, 8, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        complain(mod, PTIERR_CUDA_ERROR + (int)e, __FILE__, __LINE__, cudaGetErrorString(e));
+        return nan;
+    }
+    return h;
+}
+
+// sum_r lambda_r sum_i A_{N-1}[i, r] M[i, r], with M = mats[nmodes] the last
+// MTTKRP output (src/ktensor/ktensor.c:152-240), FP64.
+template <class Mat>
+double kruskal_inner(uint32_t nmodes, const float *lambda, Mat **mats, const char *mod)
+{
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    if (!mats || !lambda || nmodes < 1 || !mats[nmodes - 1] || !mats[nmodes] ||
+        mats[nmodes - 1]->ncols != mats[nmodes]->ncols || mats[nmodes - 1]->stride != mats[nmodes]->stride) {
+        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "bad factor or MTTKRP matrix");
+        return nan;
+    }
+    const uint32_t I = mats[nmodes - 1]->nrows, R = mats[nmodes - 1]->ncols, stride = mats[nmodes - 1]->stride;
+    if (I == 0 || R == 0) return 0.0;
+    cudaStream_t s = sync_stream();
+    DevBuf A, M, lam, out;
+    double h = nan;
+    if (A.alloc(padded((size_t)I * stride * 4), s) != cudaSuccess ||
+        M.alloc(padded((size_t)I * stride * 4), s) != cudaSuccess || lam.alloc(padded((size_t)R * 4), s) != cudaSuccess ||
+        out.alloc(64, s) != cudaSuccess) {
+        complain(mod, PTIERR_CUDA_ERROR, __FILE__, __LINE__, "device allocation failed");
+        return nan;
+    }
+    cudaMemcpyAsync(A.ptr, mats[nmodes - 1]->values, (size_t)I * stride * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(M.ptr, mats[nmodes]->values, (size_t)I * stride * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(lam.ptr, lambda, (size_t)R * 4, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(out.ptr, 0, 8, s);
+    inner_kernel<<<rows_grid_for((uint64_t)I * stride), 256, 0, s>>>(A.as<float>(), M.as<float>(), I, R, stride,
+                                                                     lam.as<float>(), out.as<double>());
+    cudaMemcpyAsync(&h, out.ptr, 8, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        complain(mod, PTIERR_CUDA_ERROR + (int)e, __FILE__, __LINE__, cudaGetErrorString(e));
+        return nan;
+    }
+    return h;
+}
+
+// fit = 1 - sqrt(||X||^2 + norm - 2 inner) / ||X|| (src/ktensor/ktensor.c:77-99,
+// the square root skipped when the residual is not positive)
+double fit_from(double normX2, double norm_mats, double inner)
+{
+    double residual = normX2 + norm_mats - 2.0 * inner;
+    if (residual > 0.0) residual = std::sqrt(residual);
+    return 1.0 - residual / std::sqrt(normX2);
+}
+
+// The reference's ALS step on caller-seeded factors (CpdAlsStep,
+// src/sptensor/cpd.c:32-160, and its HiCOO twin src/sptensor/hicoo/cpd.c:31):
+// mats[0..N-1] hold the initial factors and receive the result (unit-norm
+// columns, GetFinalLambda applied), lambda the weights, mats[N] the last
+// MTTKRP output (mode N-1 of the last iteration).  Returns the last fit, NaN
+// on error (last error set).
+template <class Mat>
+double cpd_step(ptiB200Tensor &t, uint32_t rank, uint32_t niters, double tol, Mat **mats, float *lambda,
+                const char *mod)
+{
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    const uint32_t N = t.nmodes;
+    auto fail = [&](const char *why) {
+        complain(mod, PTIERR_SHAPE_MISMATCH, __FILE__, __LINE__, why);
+        return nan;
+    };
+    if (!mats || !lambda) return fail("null factors or lambda");
+    for (uint32_t m = 0; m <= N; ++m)
+        if (!mats[m] || !mats[m]->values) return fail("null factor matrix");
+    const uint32_t stride = mats[0]->stride;
+    for (uint32_t m = 0; m < N; ++m)
+        if (mats[m]->nrows != t.ndims[m] || (uint32_t)mats[m]->ncols != rank || (uint32_t)mats[m]->stride != stride)
+            return fail("factor m must be ndims[m] x rank, all with one stride");
+    if ((uint32_t)mats[N]->stride != stride || std::max<uint32_t>(mats[N]->cap, mats[N]->nrows) < t.ndims[N - 1])
+        return fail("mats[nmodes] must hold ndims[nmodes-1] rows of the factors' stride");
+    cudaStream_t s = sync_stream();
+    DevBuf A[kMaxModes], lam, Mlast;
+    float *ptrs[kMaxModes];
+    for (uint32_t m = 0; m < N; ++m) {
+        const size_t n = (size_t)t.ndims[m] * stride;
+        if (A[m].alloc(padded(std::max<size_t>(n, 1) * 4), s) != cudaSuccess ||
+            (n && cudaMemcpyAsync(A[m].ptr, mats[m]->values, n * 4, cudaMemcpyHostToDevice, s) != cudaSuccess))
+            return fail("device copy of the factors failed");
+        ptrs[m] = A[m].as<float>();
+    }
+    if (lam.alloc(padded((size_t)rank * 4), s) != cudaSuccess ||
+        Mlast.alloc(padded(std::max<size_t>(1, (size_t)t.ndims[N - 1] * stride) * 4), s) != cudaSuccess)
+        return fail("device allocation failed");
+    CpdOptions opt;
+    opt.R = rank;
+    opt.niters = niters;
+    opt.tol = tol;
+    opt.m_last = Mlast.as<float>();
+    CpdResult res;
+    if (cpd_device(&t, ptrs, stride, lam.as<float>(), opt, res, s) != 0) return nan;
+    for (uint32_t m = 0; m < N; ++m)
+        if (t.ndims[m])
+            cudaMemcpyAsync(mats[m]->values, A[m].ptr, (size_t)t.ndims[m] * stride * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(lambda, lam.ptr, (size_t)rank * 4, cudaMemcpyDeviceToHost, s);
+    if (res.iters && t.ndims[N - 1]) {
+        cudaMemcpyAsync(mats[N]->values, Mlast.ptr, (size_t)t.ndims[N - 1] * stride * 4, cudaMemcpyDeviceToHost, s);
+        mats[N]->nrows = t.ndims[N - 1];
+    }
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        complain(mod, PTIERR_CUDA_ERROR + (int)e, __FILE__, __LINE__, cudaGetErrorString(e));
+        return nan;
+    }
+    return res.iters ? res.fits.back() : 0.0;
+}
+
+double cpd_step_coo(const ptiSparseTensor *X, uint32_t rank, uint32_t niters, double tol, ptiMatrix **mats,
+                    float *lambda)
+{
+    const char *mod = "CpdAlsStep";
+    if (!X) {
+        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "null tensor");
+        return std::numeric_limits<double>::quiet_NaN();
+    }
+    ptiB200Tensor t;
+    if (upload_coo(&t, X, sync_stream()) != 0) return std::numeric_limits<double>::quiet_NaN();
+    return cpd_step(t, rank, niters, tol, mats, lambda, mod);
+}
+
+double cpd_step_hicoo(const ptiSparseTensorHiCOO *H, uint32_t rank, uint32_t niters, double tol, ptiRankMatrix **mats,
+                      float *lambda)
+{
+    const char *mod = "CpdAlsStepHiCOO";
+    if (!H) {
+        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "null tensor");
+        return std::numeric_limits<double>::quiet_NaN();
+    }
+    ptiB200Tensor t;
+    if (upload_hicoo(&t, H, sync_stream()) != 0) return std::numeric_limits<double>::quiet_NaN();
+    return cpd_step(t, rank, niters, tol, mats, lambda, mod);
+}
+
+double normsq_values(const float *vals, uint64_t nnz, const char *mod)
+{
+    if (nnz == 0) return 0.0;
+    cudaStream_t s = sync_stream();
+    DevBuf v, acc;
+    double h = std::numeric_limits<double>::quiet_NaN();
+    if (!vals || v.alloc(padded(nnz * 4), s) != cudaSuccess || acc.alloc(64, s) != cudaSuccess) {
+        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "null values or device allocation failed");
+        return h;
+    }
+    cudaMemcpyAsync(v.ptr, vals, nnz * 4, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(acc.ptr, 0, 8, s);
+    sumsq_kernel<<<rows_grid_for(nnz), 256, 0, s>>>(v.as<float>(), nnz, acc.as<double>());
+    cudaMemcpyAsync(&h, acc.ptr, 8, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        complain(mod, PTIERR_CUDA_ERROR + (int)e, __FILE__, __LINE__, cudaGetErrorString(e));
+        return std::numeric_limits<double>::quiet_NaN();
+    }
+    return h;
+}
+
+}  // namespace
 }  // namespace
 }  // namespace pti
 
@@ -697,19 +1167,123 @@ int ptiB200CpdAlsCheckpoint(ptiB200Tensor *t, ptiIndex rank, ptiIndex niters, do
 
 double SparseTensorFrobeniusNormSquared(ptiSparseTensor const *const ptien)
 {
+    return ptien ? pti::normsq_values(ptien->values.data, ptien->nnz, "SparseTensorFrobeniusNormSquared") : 0.0;
+}
+
+double SparseTensorFrobeniusNormSquaredHiCOO(ptiSparseTensorHiCOO const *const hitsr)
+{
+    return hitsr ? pti::normsq_values(hitsr->values.data, hitsr->nnz, "SparseTensorFrobeniusNormSquaredHiCOO") : 0.0;
+}
+
+int ptiMatrixDotMulSeqTriangle(ptiIndex const mode, ptiIndex const nmodes, ptiMatrix **mats)
+{
+    return pti::normals<ptiMatrix>(mode, nmodes, mats, nullptr, "ptiMatrixDotMulSeqTriangle");
+}
+int ptiRankMatrixDotMulSeqTriangle(ptiIndex const mode, ptiIndex const nmodes, ptiRankMatrix **mats)
+{
+    return pti::normals<ptiRankMatrix>(mode, nmodes, mats, nullptr, "ptiRankMatrixDotMulSeqTriangle");
+}
+int ptiMatrixSolveNormals(ptiIndex const mode, ptiIndex const nmodes, ptiMatrix **aTa, ptiMatrix *rhs)
+{
     using namespace pti;
-    if (!ptien || ptien->nnz == 0) return 0.0;
-    cudaStream_t s = sync_stream();
-    DevBuf v, acc;
-    double h = 0.0;
-    if (v.alloc(padded(ptien->nnz * 4), s) != cudaSuccess || acc.alloc(64, s) != cudaSuccess) return -1.0;
-    cudaMemcpyAsync(v.ptr, ptien->values.data, ptien->nnz * 4, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(acc.ptr, 0, 8, s);
-    sumsq_kernel<<<(unsigned)std::min<uint64_t>((ptien->nnz + 255) / 256, (uint64_t)sm_count() * 8), 256, 0, s>>>(
-        v.as<float>(), ptien->nnz, acc.as<double>());
-    cudaMemcpyAsync(&h, acc.ptr, 8, cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    return h;
+    PTI_CHECK(rhs, PTIERR_VALUE_ERROR, "ptiMatrixSolveNormals", "null right-hand side");
+    return normals<ptiMatrix>(mode, nmodes, aTa, rhs, "ptiMatrixSolveNormals");
+}
+int ptiRankMatrixSolveNormals(ptiIndex const mode, ptiIndex const nmodes, ptiRankMatrix **aTa, ptiRankMatrix *rhs)
+{
+    using namespace pti;
+    PTI_CHECK(rhs, PTIERR_VALUE_ERROR, "ptiRankMatrixSolveNormals", "null right-hand side");
+    return normals<ptiRankMatrix>(mode, nmodes, aTa, rhs, "ptiRankMatrixSolveNormals");
+}
+int ptiMatrix2Norm(ptiMatrix *const A, ptiValue *const lambda)
+{
+    return pti::col_normalize(A, lambda, 1, "ptiMatrix2Norm");
+}
+int ptiRankMatrix2Norm(ptiRankMatrix *const A, ptiValue *const lambda)
+{
+    return pti::col_normalize(A, lambda, 1, "ptiRankMatrix2Norm");
+}
+int ptiMatrixMaxNorm(ptiMatrix *const A, ptiValue *const lambda)
+{
+    return pti::col_normalize(A, lambda, 0, "ptiMatrixMaxNorm");
+}
+int ptiRankMatrixMaxNorm(ptiRankMatrix *const A, ptiValue *const lambda)
+{
+    return pti::col_normalize(A, lambda, 0, "ptiRankMatrixMaxNorm");
+}
+void GetFinalLambda(ptiIndex const rank, ptiIndex const nmodes, ptiMatrix **mats, ptiValue *const lambda)
+{
+    pti::final_lambda(rank, nmodes, mats, lambda, "GetFinalLambda");
+}
+void GetRankFinalLambda(ptiElementIndex const rank, ptiIndex const nmodes, ptiRankMatrix **mats,
+                        ptiValue *const lambda)
+{
+    pti::final_lambda<ptiRankMatrix>(rank, nmodes, mats, lambda, "GetRankFinalLambda");
+}
+
+double KruskalTensorFrobeniusNormSquared(ptiIndex const nmodes, ptiValue const *const lambda, ptiMatrix **ata)
+{
+    return pti::kruskal_normsq(nmodes, lambda, ata, "KruskalTensorFrobeniusNormSquared");
+}
+double KruskalTensorFrobeniusNormSquaredRank(ptiIndex const nmodes, ptiValue const *const lambda, ptiRankMatrix **ata)
+{
+    return pti::kruskal_normsq(nmodes, lambda, ata, "KruskalTensorFrobeniusNormSquaredRank");
+}
+double SparseKruskalTensorInnerProduct(ptiIndex const nmodes, ptiValue const *const lambda, ptiMatrix **mats)
+{
+    return pti::kruskal_inner(nmodes, lambda, mats, "SparseKruskalTensorInnerProduct");
+}
+double SparseKruskalTensorInnerProductRank(ptiIndex const nmodes, ptiValue const *const lambda, ptiRankMatrix **mats)
+{
+    return pti::kruskal_inner(nmodes, lambda, mats, "SparseKruskalTensorInnerProductRank");
+}
+double KruskalTensorFit(ptiSparseTensor const *const ptien, ptiValue const *const lambda, ptiMatrix **mats,
+                        ptiMatrix **ata)
+{
+    if (!ptien) return std::numeric_limits<double>::quiet_NaN();
+    const uint32_t N = ptien->nmodes;
+    return pti::fit_from(SparseTensorFrobeniusNormSquared(ptien), KruskalTensorFrobeniusNormSquared(N, lambda, ata),
+                         SparseKruskalTensorInnerProduct(N, lambda, mats));
+}
+double KruskalTensorFitHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiValue const *const lambda,
+                             ptiRankMatrix **mats, ptiRankMatrix **ata)
+{
+    if (!hitsr) return std::numeric_limits<double>::quiet_NaN();
+    const uint32_t N = hitsr->nmodes;
+    return pti::fit_from(SparseTensorFrobeniusNormSquaredHiCOO(hitsr),
+                         KruskalTensorFrobeniusNormSquaredRank(N, lambda, ata),
+                         SparseKruskalTensorInnerProductRank(N, lambda, mats));
+}
+
+double CpdAlsStep(ptiSparseTensor const *const ptien, ptiIndex const rank, ptiIndex const niters, double const tol,
+                  ptiMatrix **mats, ptiValue *const lambda)
+{
+    return pti::cpd_step_coo(ptien, rank, niters, tol, mats, lambda);
+}
+double OmpCpdAlsStep(ptiSparseTensor const *const ptien, ptiIndex const rank, ptiIndex const niters, double const tol,
+                     const int tk, const int use_reduce, ptiMatrix **mats, ptiMatrix **copy_mats,
+                     ptiValue *const lambda)
+{
+    (void)tk;
+    (void)use_reduce;
+    (void)copy_mats;
+    return pti::cpd_step_coo(ptien, rank, niters, tol, mats, lambda);
+}
+double CpdAlsStepHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiIndex const rank, ptiIndex const niters,
+                       double const tol, ptiRankMatrix **mats, ptiValue *const lambda)
+{
+    return pti::cpd_step_hicoo(hitsr, rank, niters, tol, mats, lambda);
+}
+double OmpCpdAlsStepHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiIndex const rank, ptiIndex const niters,
+                          double const tol, const int tk, const int tb, const int *par_iters, ptiRankMatrix **mats,
+                          ptiRankMatrix ***copy_mats, ptiValue *const lambda, int balanced)
+{
+    (void)tk;
+    (void)tb;
+    (void)par_iters;
+    (void)copy_mats;
+    (void)balanced;
+    return pti::cpd_step_hicoo(hitsr, rank, niters, tol, mats, lambda);
 }
 
 }  // extern "C"

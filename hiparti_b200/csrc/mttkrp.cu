@@ -642,6 +642,63 @@ int ptiCudaMTTKRPOneKernel(ptiSparseTensor const *const X, ptiMatrix **const mat
     (void)impl_num;
     return pti::mttkrp_host_coo(X, mats, mats_order, mode);
 }
+int ptiCudaMTTKRPDevice(const ptiIndex mode, const ptiIndex nmodes, const ptiNnzIndex nnz, const ptiIndex rank,
+                        const ptiIndex stride, const ptiIndex *Xndims, ptiIndex **const Xinds, const ptiValue *Xvals,
+                        const ptiIndex *dev_mats_order, ptiValue **dev_mats, ptiValue *dev_scratch)
+{
+    using namespace pti;
+    (void)Xndims;
+    (void)dev_scratch;
+    const char *mod = "CUDA SpTns MTTKRP (device)";
+    PTI_CHECK(nmodes >= 2 && nmodes <= (uint32_t)kMaxModes && mode < nmodes, PTIERR_VALUE_ERROR, mod,
+              "unsupported number of modes or mode out of range");
+    PTI_CHECK(rank >= 1 && stride >= rank && stride % 4 == 0, PTIERR_SHAPE_MISMATCH, mod,
+              "stride must be >= rank and a multiple of 4");
+    if (nnz == 0) return 0;
+    PTI_CHECK(Xinds && Xvals && dev_mats_order && dev_mats, PTIERR_VALUE_ERROR, mod, "null device array");
+    // the pointer arrays and the mode order live in device memory, as the
+    // reference's kernel reads them there (mttkrp_cuda_kernels.cu:374-427)
+    cudaStream_t s = sync_stream();
+    std::vector<ptiIndex *> inds(nmodes);
+    std::vector<ptiValue *> mats(nmodes + 1);
+    std::vector<ptiIndex> order(nmodes);
+    PTI_CUDA(cudaMemcpyAsync(inds.data(), Xinds, nmodes * sizeof(ptiIndex *), cudaMemcpyDeviceToHost, s), mod);
+    PTI_CUDA(cudaMemcpyAsync(mats.data(), dev_mats, (nmodes + 1) * sizeof(ptiValue *), cudaMemcpyDeviceToHost, s),
+             mod);
+    PTI_CUDA(cudaMemcpyAsync(order.data(), dev_mats_order, nmodes * sizeof(ptiIndex), cudaMemcpyDeviceToHost, s),
+             mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    uint32_t seen = 0;
+    for (uint32_t i = 0; i < nmodes; ++i) {
+        PTI_CHECK(order[i] < nmodes && !(seen >> order[i] & 1u), PTIERR_VALUE_ERROR, mod,
+                  "mats_order must be a permutation of the modes");
+        seen |= 1u << order[i];
+    }
+    PTI_CHECK(order[0] == mode, PTIERR_VALUE_ERROR, mod, "mats_order[0] must equal mode");
+    PTI_CHECK(mats[nmodes] && ((uintptr_t)mats[nmodes] & 15) == 0, PTIERR_VALUE_ERROR, mod,
+              "output must be non-null and 16-byte aligned");
+    CooArgs a{};
+    a.nnz = nnz;
+    a.nin = nmodes - 1;
+    a.R = rank;
+    a.stride = stride;
+    a.out_ind = inds[mode];
+    for (uint32_t i = 1; i < nmodes; ++i) {
+        const uint32_t k = order[i];
+        PTI_CHECK(inds[k] && mats[k] && ((uintptr_t)mats[k] & 15) == 0, PTIERR_VALUE_ERROR, mod,
+                  "factors must be non-null and 16-byte aligned");
+        a.in_ind[i - 1] = inds[k];
+        a.in_mat[i - 1] = mats[k];
+    }
+    PTI_CHECK(a.out_ind, PTIERR_VALUE_ERROR, mod, "null index array");
+    a.vals = Xvals;
+    a.out = mats[nmodes];
+    launch_coo<float>(a, group_lanes(rank), s);
+    PTI_CUDA(cudaGetLastError(), mod);
+    PTI_CUDA(cudaStreamSynchronize(s), mod);
+    return 0;
+}
+
 int ptiMTTKRPHiCOO(ptiSparseTensorHiCOO const *const hitsr, ptiMatrix *mats[], ptiIndex const mats_order[],
                    ptiIndex const mode)
 {
@@ -848,7 +905,8 @@ std::mutex g_noalloc_mu;
 
 // Device addresses of the scratch arrays for the current device, looked up
 // once per device (host code must not use the symbols' host-side names as
-// device pointers).
+// device pointers).  They stay valid for the life of the device's primary
+// context; a cudaDeviceReset would leave them stale, which the header states.
 int noalloc_scratch(NoAllocScratch &out, const char *mod)
 {
     int dev = 0;

@@ -302,6 +302,133 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
     if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
 }
 
+// Walks records [j0, j1) of a tile whose n records s_rec are in output-row
+// order and accumulates v * prod_k A_k[row_k] one row run at a time.  Every
+// record is walkable: the decode gave a record with a bad coordinate value 0
+// and operand offsets 0, and an output row kNoRow only where its own row is
+// out of range (such records sort after every valid row), so the rows of a
+// slice never decrease and a batch whose last record continues the current
+// row lies wholly in that row.  The batch loop is therefore one compare and
+// one warp vote per U records; a row change falls to the per-record path.
+// Runs shared with neighbouring groups are merged as RunWriter does.
+template <int G, int CPL, int U, class FT, int NIN>
+__device__ __forceinline__ void walk_rows(const uint4 *s_rec, const float *s_v3, uint32_t n, uint32_t j0,
+                                          uint32_t j1, uint32_t g, uint32_t lane, const SchedArgs &a,
+                                          float *s_slots, uint32_t *s_slot_row, uint8_t *s_slot_whole)
+{
+    constexpr uint32_t kGroups = kSchedThreads / G;
+    const uint32_t col = lane * CPL;
+    const bool active = col < a.R;
+    bool first_shared = false, last_shared = false;
+    uint32_t cur = kNoRow;
+    if (j0 < j1) {
+        const uint32_t rl = s_rec[j1 - 1].x;
+        cur = s_rec[j0].x;
+        first_shared = j0 > 0 && s_rec[j0 - 1].x == cur;
+        last_shared = j1 < n && s_rec[j1].x == rl;
+        if (lane == 0) {
+            s_slot_row[g] = first_shared ? cur : kNoRow;
+            s_slot_whole[g] = cur == rl;
+        }
+    } else if (lane == 0) {
+        s_slot_row[g] = kNoRow;
+        s_slot_whole[g] = 0;
+    }
+    float *slot = s_slots + ((size_t)g * G + lane) * CPL;
+    // inactive lanes (col >= R) read column 0 and never write
+    const FT *base[NIN];
+#pragma unroll
+    for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + (active ? col : 0u);
+    float acc[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+    bool in_first = true;
+    auto flush = [&]() {
+#pragma unroll
+        for (int q = 0; q < CPL / 4; ++q)
+            if (col + 4 * q < a.R)
+                red_add4(a.out + (size_t)cur * a.stride + col + 4 * q,
+                         mask4(make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]),
+                               col + 4 * q, a.R));
+    };
+    // the run of `cur` ends before the slice does
+    auto end_run = [&]() {
+        if (in_first && first_shared) {
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) slot[c] = acc[c];
+        } else if (cur != kNoRow && active) {
+            flush();
+        }
+        in_first = false;
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
+    };
+    auto value = [&](const uint4 &r, uint32_t j) {
+        return NIN == 3 ? s_v3[j] : __uint_as_float(NIN == 2 ? r.w : r.z);
+    };
+    uint32_t j = j0;
+    for (; j + U <= j1; j += U) {
+        uint4 r[U];
+        RowPart<CPL, FT> f[U][NIN];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            r[u] = s_rec[j + u];
+            const uint32_t rr[3] = {r[u].y, r[u].z, r[u].w};
+#pragma unroll
+            for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + rr[k], 0);
+        }
+        if (__all_sync(__activemask(), r[U - 1].x == cur)) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(acc, f[u], value(r[u], j + u));
+            continue;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (r[u].x != cur) {
+                end_run();
+                cur = r[u].x;
+            }
+            accumulate<CPL, FT, NIN>(acc, f[u], value(r[u], j + u));
+        }
+    }
+    for (; j < j1; ++j) {
+        const uint4 r = s_rec[j];
+        const uint32_t rr[3] = {r.y, r.z, r.w};
+        RowPart<CPL, FT> f[NIN];
+#pragma unroll
+        for (int k = 0; k < NIN; ++k) f[k].load(base[k] + rr[k], 0);
+        if (r.x != cur) {
+            end_run();
+            cur = r.x;
+        }
+        accumulate<CPL, FT, NIN>(acc, f, value(r, j));
+    }
+    // the slice's last run: parked if it is also the first and shared with the
+    // previous group, kept for merging if it continues into the next group
+    bool owner = false;
+    if (cur != kNoRow) {
+        if (in_first && first_shared) {
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) slot[c] = acc[c];
+        } else if (last_shared) {
+            owner = true;
+        } else if (active) {
+            flush();
+        }
+    }
+    __syncthreads();
+    if (owner) {
+        for (uint32_t h = g + 1; h < kGroups; ++h) {
+            if (s_slot_row[h] != cur) break;
+            const float *p = s_slots + ((size_t)h * G + lane) * CPL;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) acc[c] += p[c];
+            if (!s_slot_whole[h]) break;
+        }
+        if (active) flush();
+    }
+}
+
 template <int NIN, int CPL>
 struct HiSmem {
     // byte offsets inside the dynamic shared memory of hicoo_sched_kernel
@@ -334,11 +461,10 @@ struct HiSmem {
 // thread group walks a contiguous slice: a lane decodes one nonzero's output
 // and operand rows from its block coordinates and offsets, the group shares
 // them by shuffles, gathers the operand rows and accumulates row runs.
-template <int G, int CPL, class FT, int NIN>
+template <int G, int CPL, int U, class FT, int NIN>
 __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 {
     using L = HiSmem<NIN, CPL>;
-    constexpr int U = NIN == 3 || CPL == 8 ? 2 : 3;  // nonzeros in flight per group
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t s_slot_row[kSchedThreads];
@@ -401,8 +527,12 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
     s_bin += bo4;
 
     // Decode every nonzero once into a 16-byte record {output row, operand
-    // rows} (the value in the last free word, or beside the records for
-    // 4-D), written over the staged arrays once they have all been read.
+    // row offsets (row x stride)} (the value in the last free word, or beside
+    // the records for 4-D), written over the staged arrays once they have all
+    // been read.  A nonzero with a coordinate out of range sets the error
+    // word and becomes a record that adds nothing (value 0, operand rows 0);
+    // its output row is kept if that is valid, else it is kNoRow, which sorts
+    // where the schedule put it (after every valid row of the tile).
     constexpr int PER = kHiTile / kSchedThreads;
     {
         uint4 rec[PER];
@@ -413,10 +543,12 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
             rec[p] = make_uint4(kNoRow, 0u, 0u, 0u);
             vv[p] = 0.f;
             if (z < n) {
-                const uint32_t i = s_blk[z];
+                const uint32_t i0 = s_blk[z];
+                const bool ok_b = i0 < nblk;
+                const uint32_t i = ok_b ? i0 : 0u;
                 uint32_t bo, bi[3];
                 if constexpr (NIN == 3) {
-                    const uint4 q = s_bq[i < nblk ? i : 0];
+                    const uint4 q = s_bq[i];
                     bo = q.x;
                     bi[0] = q.y;
                     bi[1] = q.z;
@@ -426,22 +558,24 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 #pragma unroll
                     for (int k = 0; k < NIN; ++k) bi[k] = s_bin[k * (kHiTile + 4) + i];
                 }
-                const uint32_t o = (bo << a.sb) + s_eout[z];
+                const uint64_t o = ((uint64_t)bo << a.sb) + s_eout[z];
+                const bool ok_o = ok_b && o < a.out_dim;
                 uint32_t r[3] = {0u, 0u, 0u};
-                bool ok_z = i < nblk && o < a.out_dim;
+                bool ok_in = true;
 #pragma unroll
                 for (int k = 0; k < NIN; ++k) {
-                    r[k] = (bi[k] << a.sb) + s_ein[k * kHiTile + z];
-                    ok_z = ok_z && r[k] < a.in_dim[k];
+                    const uint64_t rk = ((uint64_t)bi[k] << a.sb) + s_ein[k * kHiTile + z];
+                    ok_in = ok_in && rk < a.in_dim[k];
+                    r[k] = (uint32_t)rk;
                 }
-                vv[p] = s_val[z];
                 // operand rows become element offsets (below 2^32: schedule_supported)
 #pragma unroll
-                for (int k = 0; k < NIN; ++k) r[k] *= a.stride;
+                for (int k = 0; k < NIN; ++k) r[k] = ok_in ? r[k] * a.stride : 0u;
+                vv[p] = ok_o && ok_in ? s_val[z] : 0.f;
                 if (NIN == 1) r[1] = __float_as_uint(vv[p]);
                 if (NIN == 2) r[2] = __float_as_uint(vv[p]);
-                rec[p] = make_uint4(ok_z ? o : kNoRow, r[0], r[1], r[2]);
-                if (!ok_z) atomicOr(a.err, 1u);
+                rec[p] = make_uint4(ok_o ? (uint32_t)o : kNoRow, r[0], r[1], r[2]);
+                if (!(ok_o && ok_in)) atomicOr(a.err, 1u);
             }
         }
         __syncthreads();
@@ -462,69 +596,10 @@ __global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
 
     const uint32_t g = tid / G, lane = tid % G;
     constexpr uint32_t kGroups = kSchedThreads / G;
-    const uint32_t col = lane * CPL;
-    const bool active = col < a.R;
     // an odd slice length puts the groups' first records on different shared-memory banks
     const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
-    bool first_shared = false, last_shared = false;
-    if (j0 < j1) {
-        const uint32_t rf = s_rec[j0].x, rl = s_rec[j1 - 1].x;
-        first_shared = j0 > 0 && s_rec[j0 - 1].x == rf;
-        last_shared = j1 < n && s_rec[j1].x == rl;
-        if (lane == 0) {
-            s_slot_row[g] = first_shared ? rf : kNoRow;
-            s_slot_whole[g] = rf == rl;
-        }
-    } else if (lane == 0) {
-        s_slot_row[g] = kNoRow;
-        s_slot_whole[g] = 0;
-    }
-    RunWriter<CPL> w(first_shared, last_shared, col, active, s_slots + ((size_t)g * G + lane) * CPL);
-    const FT *base[NIN];  // this lane's columns of each operand factor
-#pragma unroll
-    for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + col;
-    // full batches of U records without per-record bounds tests, then one
-    // partial batch
-    auto batch = [&](uint32_t j, auto check) {
-        constexpr bool CHECK = decltype(check)::value;
-        uint32_t orow[U];
-        float v[U];
-        RowPart<CPL, FT> f[U][NIN];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            orow[u] = kNoRow;
-            if (!CHECK || j + u < j1) {
-                const uint4 r = s_rec[j + u];
-                const uint32_t rr[3] = {r.y, r.z, r.w};
-                orow[u] = r.x;
-                v[u] = NIN == 3 ? s_v3[j + u] : __uint_as_float(NIN == 2 ? r.w : r.z);
-                if (orow[u] != kNoRow && active) {
-#pragma unroll
-                    for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + rr[k], 0);
-                }
-            }
-        }
-        if (same_row_batch<U>(orow, w.cur)) {  // no row bookkeeping
-            if (active) {
-#pragma unroll
-                for (int u = 0; u < U; ++u) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
-            }
-            return;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (orow[u] == kNoRow) continue;
-            w.start(orow[u], a);
-            if (active) accumulate<CPL, FT, NIN>(w.acc, f[u], v[u]);
-        }
-    };
-    uint32_t j = j0;
-    for (; j + U <= j1; j += U) batch(j, std::false_type{});
-    if (j < j1) batch(j, std::true_type{});
-    const bool owner = w.finish(a);
-    __syncthreads();
-    if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
+    walk_rows<G, CPL, U, FT, NIN>(s_rec, s_v3, n, j0, j1, g, lane, a, s_slots, s_slot_row, s_slot_whole);
 }
 
 // COO schedule: packed records sorted by output index; no sorting in the kernel.
@@ -868,7 +943,8 @@ template <int G, int CPL, class FT, int NIN>
 static int launch_hicoo(const SchedArgs &a, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = HiSmem<NIN, CPL>::total;
-    auto k = hicoo_sched_kernel<G, CPL, FT, NIN>;
+    constexpr int U = NIN == 3 || CPL == 8 ? 2 : 3;  // nonzeros in flight per group
+    auto k = hicoo_sched_kernel<G, CPL, U, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a);

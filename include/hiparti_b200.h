@@ -291,6 +291,18 @@ int ptiCudaMTTKRP(ptiSparseTensor const * const X, ptiMatrix * mats[], ptiIndex 
                   ptiIndex const mode, ptiIndex const impl_num);
 int ptiCudaMTTKRPOneKernel(ptiSparseTensor const * const X, ptiMatrix ** const mats,
                            ptiIndex * const mats_order, ptiIndex const mode, ptiIndex const impl_num);
+/* include/includes/sptensors.h:222-233, src/sptensor/mttkrp_cuda.cu:378-434:
+ * COO MTTKRP on device arrays.  Xinds (nmodes pointers), dev_mats (nmodes+1
+ * pointers) and dev_mats_order (nmodes entries) are device arrays, as are the
+ * index, value and factor arrays they point to; Xndims is not read.  The
+ * products are ADDED into dev_mats[nmodes] (rows of mode `mode`), which the
+ * caller zeroes, as in the reference.  Factors and the output: `stride`
+ * floats per row, 16-byte aligned, stride a multiple of 4.  dev_scratch (the
+ * reference's nnz x rank staging) is not used and may be NULL.  Synchronous. */
+int ptiCudaMTTKRPDevice(const ptiIndex mode, const ptiIndex nmodes, const ptiNnzIndex nnz, const ptiIndex rank,
+                        const ptiIndex stride, const ptiIndex * Xndims, ptiIndex ** const Xinds,
+                        const ptiValue * Xvals, const ptiIndex * dev_mats_order, ptiValue ** dev_mats,
+                        ptiValue * dev_scratch);
 
 /* include/includes/sptensors.h:253-257, src/sptensor/hicoo/mttkrp.c:61-310 */
 int ptiMTTKRPHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiMatrix * mats[],
@@ -341,6 +353,87 @@ int ptiCpdAlsHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank
 int ptiOmpCpdAlsHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank,
                       ptiIndex const niters, double const tol, const int tk, const int tb,
                       int balanced, ptiRankKruskalTensor * ktensor);
+
+/* The ALS step on caller-initialised factors: src/sptensor/cpd.c:32-160
+ * (CpdAlsStep), cpd_omp.c:32-178 (OmpCpdAlsStep), hicoo/cpd.c:31 and
+ * hicoo/cpd_omp.c:32-202 (HiCOO twins).  The reference exports these without
+ * declaring them in its headers.  mats[0..N-1] (ndims[m] x rank, one stride,
+ * a multiple of 8) hold the initial factors and receive the result (columns
+ * of unit 2-norm, GetFinalLambda applied); lambda (rank floats) receives the
+ * weights; mats[N] (at least ndims[N-1] rows of that stride) receives the
+ * last MTTKRP output (mode N-1 of the last iteration), as the reference
+ * leaves it.  Runs the loop of ptiCpdAls on the GPU (tol as in cpd.c:144;
+ * tk, tb, use_reduce, par_iters, balanced and copy_mats are unused).  Returns
+ * the last iteration's fit, computed from the full symmetric Grams (see
+ * KruskalTensorFit); NaN on bad arguments, with the last error set. */
+double CpdAlsStep(ptiSparseTensor const * const ptien, ptiIndex const rank, ptiIndex const niters,
+                  double const tol, ptiMatrix ** mats, ptiValue * const lambda);
+double OmpCpdAlsStep(ptiSparseTensor const * const ptien, ptiIndex const rank, ptiIndex const niters,
+                     double const tol, const int tk, const int use_reduce, ptiMatrix ** mats,
+                     ptiMatrix ** copy_mats, ptiValue * const lambda);
+double CpdAlsStepHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank, ptiIndex const niters,
+                       double const tol, ptiRankMatrix ** mats, ptiValue * const lambda);
+double OmpCpdAlsStepHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiIndex const rank,
+                          ptiIndex const niters, double const tol, const int tk, const int tb,
+                          const int * par_iters, ptiRankMatrix ** mats, ptiRankMatrix *** copy_mats,
+                          ptiValue * const lambda, int balanced);
+
+/* ---------------------------------------------------------------------------
+ * Dense ALS helpers on host matrices, run on the GPU (each copies its
+ * operands in and its results out).  Grams are rank x rank with the factors'
+ * stride; as the reference's ssyrk_('L') calls leave them, only their
+ * row-major upper triangle (i <= j) needs to be written.
+ * ------------------------------------------------------------------------ */
+/* include/includes/matrices.h:47,67, src/matrix/matrix.c:340-385:
+ * mats[nmodes] = Hadamard product, in the order mode+1, ..., mode+nmodes-1
+ * (mod nmodes), of the other Grams, FP32, written full symmetric. */
+int ptiMatrixDotMulSeqTriangle(ptiIndex const mode, ptiIndex const nmodes, ptiMatrix ** mats);
+int ptiRankMatrixDotMulSeqTriangle(ptiIndex const mode, ptiIndex const nmodes, ptiRankMatrix ** mats);
+/* include/includes/matrices.h:61-65,81-85, src/matrix/matrix_solver.c:32-83:
+ * rhs <- rhs V^{-1}, V = aTa[nmodes] = the Hadamard product above.  The solve
+ * factors V formed in FP64 from the FP32 Grams and solves in FP64 (Cholesky;
+ * Gauss-Jordan with pivoting where V is not positive definite, as the
+ * reference falls back to sgesv; a singular V leaves rhs unchanged).  rhs pad
+ * columns are written as zero.  aTa[nmodes] holds V (FP32) afterwards, where
+ * the reference leaves its Cholesky factor. */
+int ptiMatrixSolveNormals(ptiIndex const mode, ptiIndex const nmodes, ptiMatrix ** aTa, ptiMatrix * rhs);
+int ptiRankMatrixSolveNormals(ptiIndex const mode, ptiIndex const nmodes, ptiRankMatrix ** aTa,
+                              ptiRankMatrix * rhs);
+/* include/includes/matrices.h:48,55,78-79, src/matrix/matrix.c:389-553:
+ * lambda = column 2-norms (FP64 sums) / column maxima of the entries clamped
+ * to >= 1; the columns are divided by lambda. */
+int ptiMatrix2Norm(ptiMatrix * const A, ptiValue * const lambda);
+int ptiMatrixMaxNorm(ptiMatrix * const A, ptiValue * const lambda);
+int ptiRankMatrix2Norm(ptiRankMatrix * const A, ptiValue * const lambda);
+int ptiRankMatrixMaxNorm(ptiRankMatrix * const A, ptiValue * const lambda);
+/* include/includes/matrices.h:56-60,80, src/matrix/matrix.c:556-572: each
+ * factor's columns to unit 2-norm, lambda multiplied by the norms. */
+void GetFinalLambda(ptiIndex const rank, ptiIndex const nmodes, ptiMatrix ** mats, ptiValue * const lambda);
+void GetRankFinalLambda(ptiElementIndex const rank, ptiIndex const nmodes, ptiRankMatrix ** mats,
+                        ptiValue * const lambda);
+/* include/includes/ktensors.h:27-60, src/ktensor/ktensor.c:77-240,
+ * src/ktensor/rankktensor.c:76-242, src/sptensor/hicoo/hicoo.c:248-260.
+ * KruskalTensorFrobeniusNormSquared = |lambda^T (Hadamard_m ata[m]) lambda|
+ * in FP64, reading each Gram's row-major upper triangle (the reference's loop
+ * reads the other triangle, which its ssyrk_ calls never write, so its value
+ * depends on uninitialised memory); ata[nmodes] receives the FP32 product.
+ * SparseKruskalTensorInnerProduct = sum_r lambda_r sum_i
+ * mats[nmodes-1][i,r] mats[nmodes][i,r] (mats[nmodes]: the last MTTKRP
+ * output).  KruskalTensorFit = 1 - sqrt(||X||^2 + norm - 2 inner) / ||X||
+ * (the square root skipped when the residual is not positive).  NaN on bad
+ * arguments (last error set). */
+double KruskalTensorFit(ptiSparseTensor const * const ptien, ptiValue const * const lambda, ptiMatrix ** mats,
+                        ptiMatrix ** ata);
+double KruskalTensorFrobeniusNormSquared(ptiIndex const nmodes, ptiValue const * const lambda, ptiMatrix ** ata);
+double SparseKruskalTensorInnerProduct(ptiIndex const nmodes, ptiValue const * const lambda, ptiMatrix ** mats);
+double KruskalTensorFitHiCOO(ptiSparseTensorHiCOO const * const hitsr, ptiValue const * const lambda,
+                             ptiRankMatrix ** mats, ptiRankMatrix ** ata);
+double KruskalTensorFrobeniusNormSquaredRank(ptiIndex const nmodes, ptiValue const * const lambda,
+                                             ptiRankMatrix ** ata);
+double SparseKruskalTensorInnerProductRank(ptiIndex const nmodes, ptiValue const * const lambda,
+                                           ptiRankMatrix ** mats);
+/* include/includes/sptensors.h:131 (FP64 accumulation; GPU) */
+double SparseTensorFrobeniusNormSquaredHiCOO(ptiSparseTensorHiCOO const * const hitsr);
 
 /* ---------------------------------------------------------------------------
  * Extensions (no reference counterpart): device-resident tensors.
@@ -455,9 +548,15 @@ int ptiB200MTTKRPValues(ptiB200Tensor *t, const float *dev_vals, const void * co
  * on a device looks up the arrays' device addresses, so make that first call
  * before any stream capture.  All calls share the scratch: calls that overlap
  * on the GPU (other streams, other host threads) race and must be ordered by
- * the caller.  Runs asynchronously on `stream`; out-of-range coordinates are
- * skipped, not reported.  Uses the direct-atomic kernel (no per-mode schedule,
- * which would need memory). */
+ * the caller.  Runs asynchronously on `stream`.  Nothing is reported back
+ * from the device: nonzeros whose coordinates fall outside ndims are skipped,
+ * and a bptr that is not strictly increasing (or that does not end at nnz)
+ * is not detected and gives wrong results with return code 0, so validate
+ * bptr before the call where it is not trusted.  The looked-up addresses are
+ * kept for the life of the process: after cudaDeviceReset (or anything else
+ * that destroys and recreates the device's primary context) they are stale,
+ * and this entry point must not be called again in that process.  Uses the
+ * direct-atomic kernel (no per-mode schedule, which would need memory). */
 int ptiB200MTTKRPHiCOONoAlloc(ptiIndex nmodes, const ptiIndex *ndims, ptiNnzIndex nnz, ptiNnzIndex nb,
                               ptiElementIndex sb_bits, const ptiNnzIndex *dev_bptr,
                               const ptiBlockIndex * const *dev_binds,

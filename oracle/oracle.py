@@ -24,7 +24,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORC_SO = HERE / "_build" / "liborc.so"
 REF_SO = HERE / "_ref" / "libHiParTI.so"
-REF_SRC = Path(os.environ.get("HIPARTI_REF", "/root/reference"))
+# the reference checkout: $HIPARTI_REF, else a "reference" directory beside the repository
+REF_SRC = Path(os.environ.get("HIPARTI_REF", HERE.parent.parent / "reference")).resolve()
 
 
 def ensure_built(ref: bool = True) -> None:
@@ -516,6 +517,28 @@ class Ref:
                                           C.c_int(tk), C.c_int(1))
         assert rc == 0
         return out[: dims[mode]].copy()
+
+    def omp_hicoo_mttkrp_runner(self, dims, h, mats, R, tk):
+        """A callable mode -> output for repeated ptiOmpMTTKRPHiCOO(tk, tb=1)
+        calls on the same HiCOO tensor and factors, with the C structs built
+        once (so a timed loop measures the reference call alone).  Every call
+        overwrites the returned output array's first dims[mode] rows."""
+        N = len(h["binds"])
+        hs, keep = self._hicoo_struct(h, dims)
+        stride = mats[0].shape[1]
+        fac = [np.ascontiguousarray(m, np.float32) for m in mats]
+        out = np.zeros((max(dims), stride), np.float32)
+        arr, ms = self._mats(fac + [out], R)
+        orders = [np.asarray([(m + i) % N for i in range(N)], np.uint32) for m in range(N)]
+        keep.update(fac=fac, arr=arr, ms=ms, orders=orders)
+
+        def run(mode):
+            _ = keep
+            rc = self.L.ptiOmpMTTKRPHiCOO(C.byref(hs), arr, _u32p(orders[mode]), C.c_uint32(mode),
+                                          C.c_int(tk), C.c_int(1))
+            assert rc == 0
+            return out
+        return run
 
     def mttkrp_hicoo_rank(self, dims, h, mats, R, mode):
         """ptiMTTKRPHiCOO_MatrixTiling (ptiRankMatrix factors) of the reference."""

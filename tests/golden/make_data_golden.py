@@ -22,10 +22,10 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from hiparti_b200 import synth  # noqa: E402
-from oracle.oracle import Ref, ensure_built  # noqa: E402
+from oracle.oracle import REF_SRC, Ref, ensure_built  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
-DATA = Path("/root/reference/data/tensors")
+DATA = REF_SRC / "data" / "tensors"  # the reference checkout ($HIPARTI_REF)
 # (file, rank, sb, sk, sc) -- block sizes small enough that the tiny examples span several blocks
 FILES = [("3d_7.tns", 4, 1, 2, 3), ("3d-24.tns", 8, 1, 2, 3), ("3d_dense.tns", 8, 1, 2, 3),
          ("3D_12031.tns", 16, 3, 4, 6), ("4d_3_16.tns", 8, 1, 2, 3)]

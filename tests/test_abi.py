@@ -32,6 +32,26 @@ def test_library_exports_every_declared_symbol(lib):
         getattr(lib, n)  # cffi resolves each declared symbol
 
 
+def test_dropin_caller_links_against_this_library_alone(lib):
+    """The C caller built against the reference's own header
+    (tests/dropin/dropin_main.c) needs no symbol this library does not
+    export: every reference entry point it calls resolves here."""
+    import subprocess
+    binary = ROOT / "tests" / "dropin" / "_build" / "dropin"
+    if not binary.exists():
+        pytest.skip("drop-in caller not built (needs the reference's header)")
+    so = ROOT / "hiparti_b200" / "libhiparti_b200.so"
+    exported = {ln.split()[-1] for ln in subprocess.run(["nm", "-D", "--defined-only", str(so)], capture_output=True,
+                                                         text=True).stdout.splitlines() if " T " in ln}
+    undefined = {ln.split()[-1] for ln in subprocess.run(["nm", "-D", "--undefined-only", str(binary)],
+                                                          capture_output=True, text=True).stdout.splitlines()}
+    ours = {n for n in undefined if re.match(r"(pti|Kruskal|Sparse|Cpd|GetFinal|GetRank)", n)}
+    assert len(ours) >= 15, sorted(ours)
+    assert ours <= exported, sorted(ours - exported)
+    ldd = subprocess.run(["ldd", str(binary)], capture_output=True, text=True).stdout
+    assert "libhiparti_b200.so" in ldd and "not found" not in ldd and "libHiParTI" not in ldd
+
+
 def test_struct_layout_matches_reference():
     # sizes/offsets of include/includes/structs.h compiled with the reference
     # headers on x86-64 (gcc): see the reference struct definitions.
