@@ -43,6 +43,7 @@ C3_DIMS = (20_000, 20_000, 20_000, 500)
 C3_NNZ = 40_000_000
 C3_R = 32
 C3_ITERS = 50
+LOWRANK_R = 10  # rank of the C3-sized low-rank precision block (its planted rank)
 SEED = 2024
 
 
@@ -260,6 +261,69 @@ def run_cpd(args):
     coo.free()
     if t is not coo:
         t.free()
+    return out
+
+
+def run_cpd_lowrank(args):
+    """BF16 precision at the C3 size on a tensor whose fit is far from 0: a
+    4-D 20000^3x500 sparse tensor of exact CP rank 10 (each component on 45
+    rows of every mode, so about 41M nonzeros) plus N(0, 0.1^2) on the
+    nonzeros, R = 10 (the planted rank, where the ALS problem is well posed;
+    with R = 32 the surplus components leave the normal equations so
+    ill-conditioned that even FP32 and FP64 runs part ways), 50 iterations
+    from one seeded start: FP32 factors, BF16 factors with closing FP32 sweeps,
+    and the FP64 oracle; fit differences and factor match scores against the
+    oracle.  (The C3 construction samples a dense model at random
+    coordinates, which leaves a sparse tensor of high rank, so its fits are
+    near 0.)"""
+    import torch
+    from hiparti_b200 import DeviceTensor
+    from hiparti_b200.synth import sparse_lowrank_torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    inds, vals, _ = sparse_lowrank_torch(C3_DIMS, 10, 45, noise=0.1, seed=SEED + 17, device=dev)
+    nnz = vals.numel()
+    coo = DeviceTensor.from_torch_coo(C3_DIMS, inds, vals)
+    t = coo.to_hicoo(7, 10, 14)
+    t.prepare()
+    R = LOWRANK_R
+    stride = ((R - 1) // 8 + 1) * 8
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 18)
+    init = [torch.rand((d, stride), generator=g, device=dev, dtype=torch.float32) for d in C3_DIMS]
+    for a in init:
+        a[:, R:] = 0
+    out = {"workload": f"4-D 20000^3x500 sparse tensor of CP rank 10 (45 rows per component and mode) + "
+                       f"N(0,0.1^2), {nnz} nnz, R={R}, {args.cpd_iters} iterations, HICOO tensor",
+           "nnz": int(nnz), "iters": args.cpd_iters, "fp32_sweeps": args.fp32_sweeps}
+    res = {}
+    for prec in ["fp32", "bf16"]:
+        fac = [a.clone() for a in init]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lam, fits = t.cpd_als(fac, args.cpd_iters, rank=R, precision=prec,
+                              fp32_sweeps=args.fp32_sweeps if prec == "bf16" else args.cpd_iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[prec] = (fits[-1], lam.cpu().numpy(), [f[:, :R].cpu().numpy() for f in fac])
+        out[f"fit_{prec}"] = fits[-1]
+        out[f"s_per_iter_{prec}"] = round(dt / args.cpd_iters, 6)
+    out["fms_bf16_vs_fp32"] = round(factor_match_score(res["bf16"][1], res["bf16"][2], res["fp32"][1],
+                                                       res["fp32"][2]), 6)
+    if args.cpd_oracle:
+        from oracle.oracle import Orc, ensure_built
+        ensure_built(ref=False)
+        orc = Orc()
+        t0 = time.perf_counter()
+        o = orc.cpd_als(list(C3_DIMS), [i.cpu().numpy().astype(np.uint32) for i in inds], vals.cpu().numpy(),
+                        R, args.cpd_iters, [a[:, :R].cpu().numpy() for a in init])
+        out["oracle_s"] = round(time.perf_counter() - t0, 1)
+        out["fit_fp64_oracle"] = o["fit"]
+        for prec in ["fp32", "bf16"]:
+            out[f"fit_diff_{prec}"] = abs(res[prec][0] - o["fit"])
+            out[f"fms_{prec}_vs_oracle"] = round(factor_match_score(res[prec][1], res[prec][2], o["lambda_"],
+                                                                    o["factors"]), 6)
+    coo.free()
+    t.free()
     return out
 
 
@@ -516,7 +580,44 @@ def run_renumber(args):
         out["sample"] = {"nnz": int(keys.shape[0]), "kind": "reference", "cores": 1,
                          "s_reference_orderit_cpu": round(ref_s, 3), "s_ours_gpu_incl_copies": round(ours_s, 4),
                          "speedup": round(ref_s / ours_s, 1)}
+    out["bfs_like"] = run_bfs_like(inds, args.bfs_nnz)
     return out
+
+
+def run_bfs_like(inds, nnz):
+    """BFS-like renumbering (ptiIndexRenumber, renumber = 2) beside one
+    Lexi-order pass on the first `nnz` nonzeros of the C2 tensor: HiCOO block
+    counts (sb = 7) before and after each, and the time of each call.  The
+    BFS-like walk is a priority queue whose every step depends on the last, so
+    it runs on the host over vertex lists built on the GPU."""
+    import numpy as np
+    from hiparti_b200 import COOTensor, DeviceTensor
+    part = [i[:nnz].cpu().numpy().view(np.uint32).copy() for i in inds]
+    vals = np.ones(part[0].size, np.float32)
+    t = COOTensor(C2_DIMS, part, vals)
+
+    def nb_of(maps):
+        u = t.shuffled(maps) if maps is not None else COOTensor(C2_DIMS, [p.copy() for p in part], vals.copy())
+        d = DeviceTensor.from_coo(u)
+        h = d.to_hicoo(C2_SB, C2_SK, C2_SC)
+        nb = h.nb
+        h.free()
+        d.free()
+        return nb
+
+    t0 = time.perf_counter()
+    bfs = t.renumber(method="bfs")
+    bfs_s = time.perf_counter() - t0
+    t.renumber(1)  # warm-up
+    t0 = time.perf_counter()
+    lexi = t.renumber(1)
+    lexi_s = time.perf_counter() - t0
+    nb0, nb_b, nb_l = nb_of(None), nb_of(bfs), nb_of(lexi)
+    return {"workload": f"first {part[0].size} nonzeros of the C2 tensor, HiCOO sb=7", "nb_before": nb0,
+            "nb_after_bfs_like": nb_b, "nb_after_lexi_1_iteration": nb_l,
+            "nnz_per_block": {"before": round(part[0].size / nb0, 2), "bfs_like": round(part[0].size / nb_b, 2),
+                              "lexi": round(part[0].size / nb_l, 2)},
+            "s_bfs_like_incl_copies": round(bfs_s, 3), "s_lexi_gpu_incl_copies": round(lexi_s, 4)}
 
 
 INGEST_NNZ = 10_000_000
@@ -1121,6 +1222,40 @@ def cpu_baseline_block(args):
     return run_reference_sample(args)
 
 
+def summary_of(res):
+    """The headline figures of every block, compact."""
+    def pick(block, keys):
+        b = res.get(block) or {}
+        return {k: b[k] for k in keys if k in b}
+    out = {"c2_GBps": res.get("value"), "c2_ms_per_step": res.get("ms_per_step"),
+           "c2_per_mode_ms": (res.get("config") or {}).get("per_mode_ms"),
+           "roofline_frac": (res.get("roofline") or {}).get("frac"), "e2e_GBps": (res.get("e2e") or {}).get("value")}
+    c3 = res.get("cpd") or {}
+    if c3:
+        out["c3"] = {"ms_per_iter_fp32": round(1e3 * c3.get("s_per_iter_fp32", 0), 3),
+                     "ms_per_iter_bf16": round(1e3 * c3.get("s_per_iter_bf16", 0), 3),
+                     "speedup_bf16": c3.get("speedup_bf16_vs_fp32"),
+                     **{k: c3[k] for k in ("fit_fp64_oracle", "fit_diff_fp32", "fit_diff_bf16", "fms_fp32_vs_oracle",
+                                           "fms_bf16_vs_oracle") if k in c3}}
+    lr = res.get("cpd_lowrank") or {}
+    if lr:
+        out["c3_lowrank"] = {"ms_per_iter_fp32": round(1e3 * lr.get("s_per_iter_fp32", 0), 3),
+                             "ms_per_iter_bf16": round(1e3 * lr.get("s_per_iter_bf16", 0), 3),
+                             **{k: lr[k] for k in ("fit_fp64_oracle", "fit_fp32", "fit_bf16", "fit_diff_fp32",
+                                                   "fit_diff_bf16", "fms_fp32_vs_oracle", "fms_bf16_vs_oracle",
+                                                   "fms_bf16_vs_fp32") if k in lr}}
+    out["c4"] = pick("gradcp", ["ms_per_gradient"])
+    out["c5"] = pick("batched", ["ms_per_iter_fp32", "ms_per_iter_bf16", "ms_per_iter_fp32_tensor_by_tensor",
+                                 "max_fit_diff_fp32", "max_fit_diff_bf16"])
+    rn = res.get("renumber") or {}
+    if rn:
+        out["renumber"] = {k: rn.get(k) for k in ("nb_before", "nb_after")}
+        if "bfs_like" in rn:
+            out["renumber"]["bfs_like"] = {k: rn["bfs_like"].get(k) for k in ("nb_before", "nb_after_bfs_like",
+                                                                             "nb_after_lexi_1_iteration")}
+    return {k: v for k, v in out.items() if v not in (None, {}, [])}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1132,14 +1267,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpd", action="store_true", help="skip the CPD-ALS (C3) block")
+    ap.add_argument("--no-cpd-lowrank", action="store_true",
+                    help="skip the C3-sized low-rank CPD-ALS precision block")
     ap.add_argument("--no-gradcp", action="store_true", help="skip the gradient-CP (C4) block")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched CPD-ALS (C5) block")
     ap.add_argument("--batched-iters", type=int, default=C5_ITERS)
     ap.add_argument("--no-ingest", action="store_true", help="skip the tensor-ingest block")
     ap.add_argument("--no-renumber", action="store_true", help="skip the renumbering block")
+    ap.add_argument("--bfs-nnz", type=int, default=5_000_000,
+                    help="nonzeros of the C2 tensor the BFS-like renumbering block runs on")
     ap.add_argument("--no-ttm", action="store_true", help="skip the TTM block")
     ap.add_argument("--no-sk20", action="store_true", help="skip the C2 sk=20 block")
-    ap.add_argument("--only", choices=["cpd", "gradcp", "batched", "ingest", "renumber", "ttm", "cpu_paths", "sk20"],
+    ap.add_argument("--only", choices=["cpd", "cpd_lowrank", "gradcp", "batched", "ingest", "renumber", "ttm",
+                                       "cpu_paths", "sk20"],
                     default=None,
                     help="run one of the CPD blocks alone and print its JSON (for profiling captures)")
     ap.add_argument("--batched-oracle", type=int, default=16,
@@ -1167,7 +1307,7 @@ def main():
     if args.only:
         import torch
         torch.cuda.set_device(0)
-        block = {"cpd": run_cpd, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
+        block = {"cpd": run_cpd, "cpd_lowrank": run_cpd_lowrank, "gradcp": run_gradcp, "batched": run_batched, "ingest": run_ingest,
                  "renumber": run_renumber, "ttm": run_ttm, "cpu_paths": run_cpu_paths,
                  "sk20": run_c2_sk20}[args.only]
         print(json.dumps({"only": args.only, **block(args)}), flush=True)
@@ -1182,6 +1322,10 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["cpd"] = run_cpd(args)
+        if world == 1 and not args.no_cpd_lowrank:
+            import torch
+            torch.cuda.empty_cache()
+            res["cpd_lowrank"] = run_cpd_lowrank(args)
         if world == 1 and not args.no_gradcp:
             import torch
             torch.cuda.empty_cache()
@@ -1206,6 +1350,12 @@ def main():
             import torch
             torch.cuda.empty_cache()
             res["c2_sk20"] = run_c2_sk20(args)
+        # the CPD blocks, then a compact summary of every block, last on the
+        # line (a reader that keeps only the end of stdout still sees them)
+        for k in ("cpd", "cpd_lowrank"):
+            if k in res:
+                res[k] = res.pop(k)
+        res["summary"] = summary_of(res)
         print(json.dumps(res), flush=True)
     from hiparti_b200 import replicas
     replicas.shutdown(world)

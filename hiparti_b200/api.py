@@ -202,13 +202,16 @@ class COOTensor:
         check(lib().ptiSparseTensorMulVector(Y, self.c, vec, mode), "ptiSparseTensorMulVector")
         return self._semi_sparse(Y)
 
-    def renumber(self, iterations=1):
-        """Lexi-order renumbering (ptiIndexRenumber, computed on the GPU):
-        per mode, original index -> new index.  The tensor is not changed."""
+    def renumber(self, iterations=1, method="lexi", impl_num=1):
+        """Index renumbering (ptiIndexRenumber): method "lexi" (Lexi-order,
+        renumber = 1, on the GPU, `iterations` passes) or "bfs" (BFS-like,
+        renumber = 2).  Per mode, original index -> new index.  The tensor is
+        not changed."""
         maps = [np.empty(d, np.uint32) for d in self.dims]
         mp = ffi.new("ptiIndex *[]", [ffi.cast("ptiIndex *", m.ctypes.data) for m in maps])
+        renumber = {"lexi": 1, "bfs": 2}[method]
         lib().ptiClearLastError()
-        lib().ptiIndexRenumber(self.c, mp, 1, int(iterations), 7, 1, 1)
+        lib().ptiIndexRenumber(self.c, mp, renumber, int(iterations), 7, 1, int(impl_num))
         code = lib().ptiGetLastError(ffi.NULL, ffi.NULL, ffi.NULL, ffi.NULL)
         if code:
             raise PtiError(code, "ptiIndexRenumber")

@@ -98,6 +98,7 @@ struct BatchArgs {
     uint32_t *err;
     uint32_t ntasks, ntensors, niters, fp32_sweeps, cpl;
     int mixed;
+    uint64_t wait_ns;                 // bound of every dependency wait
 };
 
 __device__ __forceinline__ uint64_t global_ns()
@@ -114,11 +115,11 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
     return v;
 }
 
-// Waits until *p >= target.  Gives up (false) after kWaitNs, after 2^28
+// Waits until *p >= target.  Gives up (false) after wait_ns, after 2^28
 // polls should the timer not advance, or as soon as another wait of the
 // launch has given up (err holds kErrWait), so a failed launch ends within
 // about one wait bound instead of one per task.
-__device__ bool wait_at_least(const uint32_t *p, uint32_t target, const uint32_t *err)
+__device__ bool wait_at_least(const uint32_t *p, uint32_t target, const uint32_t *err, uint64_t wait_ns)
 {
     if (ld_acquire(p) >= target) return true;
     const uint64_t t0 = global_ns();
@@ -126,7 +127,7 @@ __device__ bool wait_at_least(const uint32_t *p, uint32_t target, const uint32_t
         __nanosleep(64);
         if (ld_acquire(p) >= target) return true;
         if ((i & 255u) == 255u &&
-            (global_ns() - t0 > kWaitNs || (*(volatile const uint32_t *)err & kErrWait))) return false;
+            (global_ns() - t0 > wait_ns || (*(volatile const uint32_t *)err & kErrWait))) return false;
     }
     return false;
 }
@@ -395,9 +396,12 @@ __device__ __forceinline__ void gram_row(double (&g)[kBMaxRank], float v, uint32
     }
 }
 
-// The mode-m ALS step of one tensor (one CTA).
+// The mode-m ALS step of one tensor (one CTA).  With gram_bf16 (the
+// iterations whose MTTKRPs gather BF16 factors) the new Gram is formed from
+// the BF16-rounded factor, the values those gathers read, so that the next
+// steps' right-hand sides and normal matrices come from the same factors.
 __device__ void dense_task(const BatchTensor *__restrict__ gt, uint32_t b, uint32_t m, uint32_t it,
-                           const BatchArgs &a, unsigned char *sm)
+                           const BatchArgs &a, unsigned char *sm, bool gram_bf16)
 {
     double *V = reinterpret_cast<double *>(sm + DenseSmem::V);
     double *Lm = reinterpret_cast<double *>(sm + DenseSmem::L);
@@ -542,16 +546,16 @@ __device__ void dense_task(const BatchTensor *__restrict__ gt, uint32_t b, uint3
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const uint32_t row = blk * 8 + q;
-                if (colok) {
-                    v[q] = v[q] / lam;
-                    if (row < I) {
-                        A[(size_t)row * stride + lane] = v[q];
-                        if (last) inner += (double)lam * (double)v[q] * (double)mm[q];
-                    }
+                if (colok) v[q] = v[q] / lam;
+                const __nv_bfloat16 h = __float2bfloat16_rn(colok ? v[q] : 0.f);
+                // the value the next MTTKRPs gather (and the fit's model uses)
+                const double used = gram_bf16 ? (double)__bfloat162float(h) : (double)v[q];
+                if (colok && row < I) {
+                    A[(size_t)row * stride + lane] = v[q];
+                    if (last) inner += (double)lam * used * (double)mm[q];
                 }
-                if (a.mixed && lane < stride && row < I)
-                    Ab[(size_t)row * stride + lane] = __float2bfloat16_rn(colok ? v[q] : 0.f);
-                tile[q * kRowPad + lane] = (double)v[q];
+                if (a.mixed && lane < stride && row < I) Ab[(size_t)row * stride + lane] = h;
+                tile[q * kRowPad + lane] = used;
             }
             __syncwarp();
 #pragma unroll
@@ -641,15 +645,15 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
         const bool dense = task.x & 1u;
         const uint32_t pid = task.x >> 1, b = pid / 3, m = pid % 3;
         if (tid == 0) {
-            bool ok = wait_at_least(dense_done + b, m, a.err);
-            if (ok && dense) ok = wait_at_least(tiles_done + pid, __ldg(&a.plans[pid].ntiles), a.err);
+            bool ok = wait_at_least(dense_done + b, m, a.err, a.wait_ns);
+            if (ok && dense) ok = wait_at_least(tiles_done + pid, __ldg(&a.plans[pid].ntiles), a.err, a.wait_ns);
             __threadfence();
             if (!ok) atomicOr(a.err, kErrWait);
             s_ok = ok;
         }
         __syncthreads();
         if (s_ok) {
-            if (dense) dense_task(a.tens + b, b, m, it, a, sm);
+            if (dense) dense_task(a.tens + b, b, m, it, a, sm, sizeof(FT) == 2);
             else if (copies_ok) copies_ok = tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err);
         }
         // shared memory written by this task may next be filled by bulk copies
@@ -664,8 +668,10 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
 
 __global__ void bump_kernel(uint32_t *iter) { *iter += 1; }
 
-// Grams of the initial factors and their BF16 copies; one CTA per (tensor, mode).
-__global__ void __launch_bounds__(kBThreads) batch_init_kernel(const BatchTensor *tens, int mixed)
+// Grams of the current factors and their BF16 copies; one CTA per (tensor,
+// mode).  With round_bf16 the Grams are of the BF16-rounded factors (the
+// values the BF16 iterations gather, see dense_task).
+__global__ void __launch_bounds__(kBThreads) batch_init_kernel(const BatchTensor *tens, int mixed, int round_bf16)
 {
     __shared__ double Gs[kBMaxRank * kBMaxRank];
     const BatchTensor *gt = tens + blockIdx.x / 3;
@@ -682,8 +688,9 @@ __global__ void __launch_bounds__(kBThreads) batch_init_kernel(const BatchTensor
     for (uint32_t i = warp; i < I; i += kBThreads / 32) {
         const size_t e = (size_t)i * stride + lane;
         const float v = lane < R ? A[e] : 0.f;
-        if (mixed && lane < stride) Ab[e] = __float2bfloat16_rn(v);
-        gram_row(g, v, R);
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        if (mixed && lane < stride) Ab[e] = h;
+        gram_row(g, round_bf16 ? __bfloat162float(h) : v, R);
     }
     if (lane < R) {
 #pragma unroll
@@ -949,6 +956,7 @@ int batch_iterate(ptiB200Batch *bt, uint32_t niters, int mixed, uint32_t fp32_sw
     a.fp32_sweeps = fp32_sweeps;
     a.cpl = (uint32_t)cpl;
     a.mixed = mixed;
+    a.wait_ns = kWaitNs;
     const uint32_t n16 = mixed && niters > fp32_sweeps ? niters - fp32_sweeps : 0, n32 = niters - n16;
     cudaGraphExec_t g16 = nullptr, g32 = nullptr;
     int r = 0;
@@ -962,6 +970,10 @@ int batch_iterate(ptiB200Batch *bt, uint32_t niters, int mixed, uint32_t fp32_sw
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
         for (uint32_t i = 0; i < n16 && lerr == cudaSuccess; ++i) lerr = cudaGraphLaunch(g16, s);
+        if (n16 && n32 && lerr == cudaSuccess) {  // the FP32 sweeps start from Grams of the FP32 factors
+            batch_init_kernel<<<3 * bt->B, kBThreads, 0, s>>>(bt->tens.as<BatchTensor>(), mixed, 0);
+            lerr = cudaGetLastError();
+        }
         for (uint32_t i = 0; i < n32 && lerr == cudaSuccess; ++i) lerr = cudaGraphLaunch(g32, s);
         cudaEventRecord(e1, s);
         const cudaError_t serr = cudaStreamSynchronize(s);
@@ -982,11 +994,13 @@ int batch_iterate(ptiB200Batch *bt, uint32_t niters, int mixed, uint32_t fp32_sw
     return 0;
 }
 
-int batch_init_factors(ptiB200Batch *bt, int mixed)
+// round_bf16: the first iterations gather BF16 factors (their Grams are of
+// the rounded values)
+int batch_init_factors(ptiB200Batch *bt, int mixed, int round_bf16)
 {
     cudaStream_t s = bt->s;
     PTI_CUDA(cudaMemsetAsync(bt->M.ptr, 0, bt->elems * 4, s), kMod);
-    batch_init_kernel<<<3 * bt->B, kBThreads, 0, s>>>(bt->tens.as<BatchTensor>(), mixed);
+    batch_init_kernel<<<3 * bt->B, kBThreads, 0, s>>>(bt->tens.as<BatchTensor>(), mixed, round_bf16);
     PTI_CUDA(cudaGetLastError(), kMod);
     return 0;
 }
@@ -1154,7 +1168,7 @@ int ptiB200BatchCreate(ptiB200Batch **out, ptiIndex ntensors, const ptiIndex *nd
             PTI_TRY(batch_build_plans(bt.get(), sb));
             for (int cpl : {4, 8}) {
                 batch_fill_kernel<<<sm_count() * 4, 256, 0, s>>>(bt->A.as<float>(), elems);
-                PTI_TRY(batch_init_factors(bt.get(), 1));
+                PTI_TRY(batch_init_factors(bt.get(), 1, 1));
                 float ms = 0.f;
                 PTI_TRY(batch_iterate(bt.get(), 2, 1, 1, cpl, fits.as<double>(), &ms));  // warm-up
                 PTI_TRY(batch_iterate(bt.get(), 2, 1, 1, cpl, fits.as<double>(), &ms));
@@ -1197,6 +1211,48 @@ int ptiB200BatchInfo(const ptiB200Batch *bt, int *sb_bits, int *cols_per_lane, f
     return 0;
 }
 
+int ptiB200BatchWaitProbe(ptiB200Batch *bt, double wait_seconds)
+{
+    using namespace pti;
+    PTI_CHECK(bt && bt->B >= 1, PTIERR_VALUE_ERROR, kMod, "empty batch");
+    PTI_CHECK(wait_seconds > 0.0 && wait_seconds <= 2.0, PTIERR_VALUE_ERROR, kMod,
+              "wait bound must be in (0, 2] seconds");
+    cudaStream_t s = bt->s;
+    // one task: the mode-1 dense step of tensor 0, which waits for the mode-0
+    // dense step -- a task this queue does not hold, so the counter it waits
+    // on stays 0 and the wait must give up after its bound
+    DevBuf task;
+    PTI_CUDA(task.alloc(64, s), kMod);
+    const uint2 t = make_uint2((1u << 1) | 1u, 0u);
+    PTI_CUDA(cudaMemcpyAsync(task.ptr, &t, sizeof t, cudaMemcpyHostToDevice, s), kMod);
+    uint32_t *misc = bt->misc.as<uint32_t>();
+    PTI_CUDA(cudaMemsetAsync(misc, 0, 8, s), kMod);
+    PTI_CUDA(cudaMemsetAsync(bt->ctrl.ptr, 0, (1 + 4 * (size_t)bt->B) * 4, s), kMod);
+    BatchArgs a{};
+    a.tasks = task.as<uint2>();
+    a.plans = bt->plans.as<BatchPlan>();
+    a.tens = bt->tens.as<BatchTensor>();
+    a.ctrl = bt->ctrl.as<uint32_t>();
+    a.iter = misc;
+    a.fits = nullptr;
+    a.err = misc + 1;
+    a.ntasks = 1;
+    a.ntensors = bt->B;
+    a.niters = 1;
+    a.cpl = 4;
+    a.wait_ns = (uint64_t)(wait_seconds * 1e9);
+    uint32_t grid = 0;
+    PTI_TRY(batch_grid(bt, batch_kernel(4, false), &grid));
+    batch_kernel(4, false)<<<1, kBThreads, kBatchSmem, s>>>(a);
+    PTI_CUDA(cudaGetLastError(), kMod);
+    PTI_CUDA(cudaStreamSynchronize(s), kMod);
+    uint32_t err = 0;
+    PTI_CUDA(cudaMemcpy(&err, misc + 1, 4, cudaMemcpyDeviceToHost), kMod);
+    PTI_CUDA(cudaMemsetAsync(misc, 0, 8, s), kMod);
+    PTI_CHECK(err == 0, PTIERR_CUDA_ERROR, kMod, "a work-queue or copy wait timed out");
+    return 0;
+}
+
 int ptiB200BatchCpdAls(ptiB200Batch *bt, ptiIndex niters, int precision, ptiIndex fp32_sweeps,
                        float *const *dev_factors, float *const *dev_lambda, double *fits, float *ms_per_iter,
                        void *stream)
@@ -1230,7 +1286,7 @@ int ptiB200BatchCpdAls(ptiB200Batch *bt, ptiIndex niters, int precision, ptiInde
     PTI_CUDA(cudaMemcpyAsync(bt->copies.ptr, items.data(), 3 * (size_t)B * sizeof(CopyItem), cudaMemcpyHostToDevice,
                              s), kMod);
     batch_copy_kernel<<<3 * B, 256, 0, s>>>(bt->copies.as<CopyItem>());
-    PTI_TRY(batch_init_factors(bt, mixed));
+    PTI_TRY(batch_init_factors(bt, mixed, mixed && niters > fp32_sweeps));
     DevBuf dfits;
     PTI_CUDA(dfits.alloc(padded((size_t)B * niters * 8), s), kMod);
     float ms = 0.f;

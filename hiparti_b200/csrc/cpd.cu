@@ -32,12 +32,17 @@ namespace pti {
 
 constexpr int kMaxCpdRank = 128;
 
-// Gram accumulation: G += A^T A over rows [0, I).  If inv_scale is given the
+// Gram accumulation: G += A^T A over rows [0, I).  If lambda is given the
 // rows are first divided column-wise by lambda (and written back); if bf16 is
-// given the (scaled) rows are also stored as BF16.  Dynamic shared memory:
-// R*R doubles of accumulator + 32*R doubles of row tile.
+// given the (scaled) rows are also stored as BF16.  With round_bf16 the Gram
+// is formed from the BF16-rounded values -- the ones the next MTTKRPs gather --
+// so that an ALS step's right-hand side and normal matrix come from the same
+// factors (with FP32 Grams beside BF16 gathers the normal equations are
+// inconsistent, and inside an ALS swamp, where they are ill-conditioned, the
+// solve amplifies that until the iteration diverges).  Dynamic shared
+// memory: R*R doubles of accumulator + 32*R doubles of row tile.
 __global__ void gram_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, const float *lambda,
-                            __nv_bfloat16 *bf16, double *G)
+                            __nv_bfloat16 *bf16, double *G, int round_bf16)
 {
     extern __shared__ double sm[];
     double *acc = sm;
@@ -59,8 +64,9 @@ __global__ void gram_kernel(float *A, uint32_t I, uint32_t R, uint32_t stride, c
                 v = v / lambda[c];
                 *p = v;
             }
-            if (bf16) bf16[(r0 + r) * stride + c] = __float2bfloat16_rn(v);
-            if (c < R) tile[r * R + c] = (double)v;
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            if (bf16) bf16[(r0 + r) * stride + c] = h;
+            if (c < R) tile[r * R + c] = round_bf16 ? (double)__bfloat162float(h) : (double)v;
         }
         __syncthreads();
         for (uint32_t e = threadIdx.x; e < RR; e += blockDim.x) {
@@ -251,15 +257,17 @@ __global__ void lambda_kernel(const double *colsq, const int *colmax, uint32_t R
     }
 }
 
-// inner += sum_i sum_r lambda_r A[i, r] M[i, r]
+// inner += sum_i sum_r lambda_r A[i, r] M[i, r]; with Ab the factor is read
+// from its BF16 copy (the values a BF16 iteration's MTTKRPs and Grams used,
+// so that the fit is that of one model)
 __global__ void inner_kernel(const float *A, const float *M, uint32_t I, uint32_t R, uint32_t stride,
-                             const float *lambda, double *inner)
+                             const float *lambda, double *inner, const __nv_bfloat16 *Ab = nullptr)
 {
     double s = 0.0;
     const uint64_t total = (uint64_t)I * stride;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t c = (uint32_t)(e % stride);
-        if (c < R) s += (double)A[e] * (double)M[e] * (double)lambda[c];
+        if (c < R) s += (double)(Ab ? __bfloat162float(Ab[e]) : A[e]) * (double)M[e] * (double)lambda[c];
     }
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(inner, s);
@@ -420,11 +428,19 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
         return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + per - 1) / per, sms * 4ull));
     };
 
-    // initial Grams (cpd.c:65-72) and BF16 copies
-    PTI_CUDA(cudaMemsetAsync(G.ptr, 0, (size_t)N * RR * 8, s), mod);
-    for (uint32_t m = 0; m < N; ++m)
-        gram_kernel<<<rows_grid(t->ndims[m], 32), 256, gram_smem, s>>>(
-            A[m], t->ndims[m], R, stride, nullptr, mixed ? Ab[m].as<__nv_bfloat16>() : nullptr, G.as<double>() + (size_t)m * RR);
+    // Grams of every factor (cpd.c:65-72) and their BF16 copies; with
+    // round_bf16 the Grams are of the BF16-rounded factors (gram_kernel)
+    auto all_grams = [&](int round_bf16) -> int {
+        PTI_CUDA(cudaMemsetAsync(G.ptr, 0, (size_t)N * RR * 8, s), mod);
+        for (uint32_t m = 0; m < N; ++m)
+            gram_kernel<<<rows_grid(t->ndims[m], 32), 256, gram_smem, s>>>(
+                A[m], t->ndims[m], R, stride, nullptr, mixed ? Ab[m].as<__nv_bfloat16>() : nullptr,
+                G.as<double>() + (size_t)m * RR, round_bf16);
+        return 0;
+    };
+    const uint32_t it_first = have_ckpt ? st.iters : 0;
+    bool grams_bf16 = mixed && it_first + opt.fp32_sweeps < opt.niters;
+    PTI_TRY(all_grams(grams_bf16));
     PTI_CUDA(cudaMemsetAsync(scal.ptr, 0, 16, s), mod);
     if (t->nnz) sumsq_kernel<<<rows_grid(t->nnz, 256), 256, 0, s>>>(t->vals.as<float>(), t->nnz, normX2);
     PTI_CUDA(cudaGetLastError(), mod);
@@ -462,6 +478,10 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
     uint32_t it = have_ckpt ? st.iters : 0;
     for (; it < opt.niters && !converged; ++it) {
         const bool use_bf16 = mixed && it + opt.fp32_sweeps < opt.niters;
+        if (use_bf16 != grams_bf16) {  // the closing FP32 sweeps start: Grams of the FP32 factors
+            grams_bf16 = use_bf16;
+            PTI_TRY(all_grams(grams_bf16));
+        }
         for (uint32_t k = 0; k < N; ++k)
             fptr[k] = use_bf16 ? (const void *)Ab[k].ptr : (const void *)A[k];
         for (uint32_t m = 0; m < N; ++m) {
@@ -485,13 +505,14 @@ int cpd_device(ptiB200Tensor *t, float *const *A, uint32_t stride, float *lambda
             PTI_CUDA(cudaMemsetAsync(G.as<double>() + (size_t)m * RR, 0, (size_t)RR * 8, s), mod);
             gram_kernel<<<rows_grid(t->ndims[m], 32), 256, gram_smem, s>>>(
                 A[m], t->ndims[m], R, stride, lambda, mixed ? Ab[m].as<__nv_bfloat16>() : nullptr,
-                G.as<double>() + (size_t)m * RR);
+                G.as<double>() + (size_t)m * RR, use_bf16);
             PTI_CUDA(cudaGetLastError(), mod);
         }
         const uint32_t last = N - 1;
         PTI_CUDA(cudaMemsetAsync(inner, 0, 8, s), mod);
         inner_kernel<<<rows_grid((uint64_t)t->ndims[last] * stride, 256), 256, 0, s>>>(
-            A[last], M.as<float>(), t->ndims[last], R, stride, lambda, inner);
+            A[last], M.as<float>(), t->ndims[last], R, stride, lambda, inner,
+            use_bf16 ? Ab[last].as<__nv_bfloat16>() : nullptr);
         fit_kernel<<<1, 256, 0, s>>>(G.as<double>(), N, R, lambda, normX2, inner, fits + it);
         PTI_CUDA(cudaGetLastError(), mod);
         if (opt.tol > 0.0) {

@@ -245,6 +245,182 @@ int lexi_order_mode(uint32_t N, const std::vector<uint32_t> &ndims, uint64_t nnz
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// BFS-like renumbering (renumber == 2): src/sptensor/renumber.c:534-839.
+//
+// The tensor is a hypergraph with a vertex per index of every mode and a
+// hyperedge per nonzero.  Mode by mode, the mode's vertices are taken from a
+// binary max-heap on a key (all 0 at first); on equal keys the heap prefers
+// the smaller degree when it sifts down and the larger degree when it sifts
+// up, as the reference's heapify and heapIncreaseKey do (:644-701).  The
+// vertex taken gets the next new index; every vertex of its hyperedges not
+// yet visited in this mode's pass is visited, and each hyperedge of that
+// vertex raises by one the key of its own vertex in the mode, if that vertex
+// is still in the heap.  Every vertex starts unvisited: the reference reads
+// the visit marks of other modes' vertices before it ever writes them
+// (renumber.c:768), so its own result depends on leftover heap memory and is
+// not reproducible; this is the reading under which the loop is the
+// maximum-cardinality search it describes.
+//
+// The vertex -> hyperedge lists are built on the GPU (a stable sort of the
+// nonzero ids by each mode's index).  The walk itself is a priority queue
+// whose every step depends on the keys the previous steps raised, so it runs
+// on the host, one heap operation at a time.
+// ---------------------------------------------------------------------------
+__global__ void widen_k(const uint32_t *src, uint64_t n, uint64_t *dst) { GRID_LOOP(i, n) dst[i] = src[i]; }
+
+// off[c] = number of keys below c, for c in [0, ncols]
+__global__ void lower_bound_k(const uint64_t *key, uint64_t n, uint32_t ncols, uint64_t *off)
+{
+    GRID_LOOP(c, (uint64_t)ncols + 1)
+    {
+        uint64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (key[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        off[c] = lo;
+    }
+}
+
+// Per mode: the nonzeros of every index, in increasing nonzero order.
+struct VertexLists {
+    std::vector<std::vector<uint32_t>> edges;  // [mode][nnz]
+    std::vector<std::vector<uint64_t>> off;    // [mode][ndims + 1]
+};
+
+int vertex_lists(uint32_t N, const uint32_t *ndims, uint64_t nnz, const uint32_t *const *host_inds, VertexLists &vl,
+                 cudaStream_t s)
+{
+    const char *mod = "B200 BFS-like renumbering";
+    PTI_CHECK(nnz < 0xFFFFFFFFull, PTIERR_VALUE_ERROR, mod, "too many nonzeros");
+    vl.edges.assign(N, {});
+    vl.off.assign(N, {});
+    uint32_t maxd = 0;
+    for (uint32_t m = 0; m < N; ++m) maxd = std::max(maxd, ndims[m]);
+    DevBuf ind, keys, vals, off;
+    RadixScratch sc;
+    if (nnz) {
+        PTI_CUDA(ind.alloc(padded(nnz * 4), s), mod);
+        PTI_CUDA(keys.alloc(padded(nnz * 8), s), mod);
+        PTI_CUDA(vals.alloc(padded(nnz * 4), s), mod);
+        PTI_TRY(sc.alloc(nnz, s));
+    }
+    PTI_CUDA(off.alloc(padded(((uint64_t)maxd + 1) * 8), s), mod);
+    for (uint32_t m = 0; m < N; ++m) {
+        vl.edges[m].resize(nnz);
+        vl.off[m].assign((size_t)ndims[m] + 1, 0);
+        if (!nnz) continue;
+        PTI_CUDA(cudaMemcpyAsync(ind.ptr, host_inds[m], nnz * 4, cudaMemcpyHostToDevice, s), mod);
+        widen_k<<<grid_n(nnz), 256, 0, s>>>(ind.as<uint32_t>(), nnz, keys.as<uint64_t>());
+        iota_k<<<grid_n(nnz), 256, 0, s>>>(vals.as<uint32_t>(), nnz);
+        PTI_TRY(radix_sort_pairs(keys, vals, nnz, ((bits_of(ndims[m] ? ndims[m] - 1 : 0) + 7) / 8) * 8, sc, s));
+        lower_bound_k<<<grid_n((uint64_t)ndims[m] + 1), 256, 0, s>>>(keys.as<uint64_t>(), nnz, ndims[m],
+                                                                     off.as<uint64_t>());
+        PTI_CUDA(cudaGetLastError(), mod);
+        PTI_CUDA(cudaMemcpyAsync(vl.edges[m].data(), vals.ptr, nnz * 4, cudaMemcpyDeviceToHost, s), mod);
+        PTI_CUDA(cudaMemcpyAsync(vl.off[m].data(), off.ptr, ((size_t)ndims[m] + 1) * 8, cudaMemcpyDeviceToHost, s),
+                 mod);
+        PTI_CUDA(cudaStreamSynchronize(s), mod);
+    }
+    return 0;
+}
+
+// The heap of one mode's pass: slots 1..size hold vertices; pos[v] is v's
+// slot (0 once taken).
+struct BfsHeap {
+    std::vector<uint32_t> slot, pos;
+    std::vector<uint64_t> key;
+    const uint64_t *off;  // degree(v) = off[v+1] - off[v]
+    uint32_t size = 0;
+    uint64_t deg(uint32_t v) const { return off[v + 1] - off[v]; }
+    // the reference's sift-down preference: larger key, then smaller degree
+    bool above_down(uint32_t a, uint32_t b) const
+    {
+        return key[a] > key[b] || (key[a] == key[b] && deg(a) < deg(b));
+    }
+    void down(uint32_t j)
+    {
+        while (j <= size / 2) {
+            const uint32_t l = 2 * j, r = 2 * j + 1;
+            uint32_t big = above_down(slot[l], slot[j]) ? l : j;
+            if (r <= size && above_down(slot[r], slot[big])) big = r;
+            if (big == j) break;
+            std::swap(slot[big], slot[j]);
+            pos[slot[big]] = big;
+            pos[slot[j]] = j;
+            j = big;
+        }
+    }
+    // raises v's key by one and sifts it up (larger key, then larger degree)
+    void raise(uint32_t v)
+    {
+        uint32_t i = pos[v];
+        if (i == 0 || i > size) return;
+        key[v] += 1;
+        while (i > 1) {
+            const uint32_t p = slot[i >> 1];
+            if (!(key[v] > key[p] || (key[v] == key[p] && deg(v) > deg(p)))) break;
+            slot[i] = p;
+            pos[p] = i;
+            i >>= 1;
+        }
+        slot[i] = v;
+        pos[v] = i;
+    }
+    uint32_t take()
+    {
+        const uint32_t v = slot[1];
+        slot[1] = slot[size];
+        pos[slot[1]] = 1;
+        --size;
+        pos[v] = 0;
+        down(1);
+        return v;
+    }
+};
+
+int bfs_like(uint32_t N, const uint32_t *ndims, uint64_t nnz, const uint32_t *const *host_inds, uint32_t **newIndices,
+             cudaStream_t s)
+{
+    VertexLists vl;
+    PTI_TRY(vertex_lists(N, ndims, nnz, host_inds, vl, s));
+    std::vector<std::vector<uint8_t>> visited(N);
+    for (uint32_t d = 0; d < N; ++d) {
+        const uint32_t n = ndims[d];
+        if (n == 0) continue;
+        BfsHeap H;
+        H.off = vl.off[d].data();
+        H.slot.resize((size_t)n + 1);
+        H.pos.resize(n);
+        H.key.assign(n, 0);
+        for (uint32_t v = 0; v < n; ++v) {
+            H.slot[v + 1] = v;
+            H.pos[v] = v + 1;
+        }
+        H.size = n;
+        for (uint32_t j = n / 2; j >= 1; --j) H.down(j);
+        for (uint32_t m = 0; m < N; ++m) visited[m].assign(m == d ? 0 : ndims[m], 0);
+        const uint32_t *mine = host_inds[d];
+        for (uint32_t t = 0; t < n; ++t) {
+            const uint32_t v = H.take();
+            newIndices[d][v] = t;
+            for (uint64_t j = vl.off[d][v]; j < vl.off[d][v + 1]; ++j) {
+                const uint32_t h = vl.edges[d][j];
+                for (uint32_t k = 0; k < N; ++k) {
+                    if (k == d) continue;
+                    const uint32_t w = host_inds[k][h];
+                    if (visited[k][w]) continue;
+                    visited[k][w] = 1;
+                    for (uint64_t jj = vl.off[k][w]; jj < vl.off[k][w + 1]; ++jj) H.raise(mine[vl.edges[k][jj]]);
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 }  // namespace
 
 // Lexi-order renumbering of a device COO tensor.  maps[m] (device, ndims[m])
@@ -306,13 +482,17 @@ int ptiB200Renumber(ptiB200Tensor *t, ptiIndex iterations, ptiIndex * const *new
     return 0;
 }
 
-// include/includes/sptensors.h:100, src/sptensor/renumber.c:26-92.  Lexi-order
-// (renumber == 1) on the GPU; tsr is left as it was.  sb_bits and tk are not
-// used; impl_num 0 and 1 both mean the exact other-mode rows (the reference
-// leaves its comparison undefined for 0).  BFS-like (renumber == 2) and the
-// row-block rows of impl_num 2 are not provided: the call records
-// PTIERR_VALUE_ERROR (read it with ptiGetLastError) and returns newIndices as
-// the identity, as it does on any other failure.
+// include/includes/sptensors.h:100, src/sptensor/renumber.c:26-92; tsr is
+// left as it was.  renumber == 1: Lexi-order on the GPU, `iterations` passes.
+// impl_num 0, 1 and 2 all mean rows of exactly equal other-mode coordinates:
+// impl_num 2 compares each mode by its block index and then its full index
+// (sort.c:890-917), which orders the coordinates exactly as comparing the
+// full indices does, and its quicksort (sort.c:1402-1431) sorts correctly, so
+// the reference's own results for 2 are orderit's.  renumber == 2: BFS-like
+// (bfs_like above; iterations and impl_num unused).  sb_bits and tk are not
+// used.  Other choices (impl_num 3, which the reference marks as not
+// working) record PTIERR_VALUE_ERROR (read it with ptiGetLastError) and
+// return newIndices as the identity, as the call does on any other failure.
 void ptiIndexRenumber(ptiSparseTensor *tsr, ptiIndex **newIndices, int renumber, ptiIndex iterations,
                       ptiElementIndex sb_bits, int tk, int impl_num)
 {
@@ -323,8 +503,23 @@ void ptiIndexRenumber(ptiSparseTensor *tsr, ptiIndex **newIndices, int renumber,
     for (ptiIndex m = 0; m < tsr->nmodes; ++m)
         for (ptiIndex i = 0; i < tsr->ndims[m]; ++i) newIndices[m][i] = i;
     const char *mod = "B200 Renumber";
-    if (renumber != 1 || (impl_num != 0 && impl_num != 1)) {
-        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__, "only Lexi-order with exact rows is provided");
+    if (renumber == 2) {
+        std::vector<const uint32_t *> hi(tsr->nmodes);
+        for (ptiIndex m = 0; m < tsr->nmodes; ++m) hi[m] = tsr->inds[m].data;
+        std::vector<std::vector<uint32_t>> out(tsr->nmodes);
+        std::vector<uint32_t *> op(tsr->nmodes);
+        for (ptiIndex m = 0; m < tsr->nmodes; ++m) {
+            out[m].resize(tsr->ndims[m]);
+            op[m] = out[m].data();
+        }
+        if (bfs_like(tsr->nmodes, tsr->ndims, tsr->nnz, hi.data(), op.data(), sync_stream()) != 0) return;
+        for (ptiIndex m = 0; m < tsr->nmodes; ++m)
+            if (tsr->ndims[m]) std::memcpy(newIndices[m], out[m].data(), (size_t)tsr->ndims[m] * 4);
+        return;
+    }
+    if (renumber != 1 || impl_num < 0 || impl_num > 2) {
+        complain(mod, PTIERR_VALUE_ERROR, __FILE__, __LINE__,
+                 "renumber must be 1 (Lexi-order, impl_num 0..2) or 2 (BFS-like)");
         return;
     }
     cudaStream_t s = sync_stream();
@@ -354,8 +549,8 @@ void ptiIndexRenumber(ptiSparseTensor *tsr, ptiIndex **newIndices, int renumber,
 }
 
 // include/includes/sptensors.h:101, src/sptensor/orderit.c:121-208: the same
-// Lexi-order (renumber == 1); BFS-like (renumber == 2) is not provided and
-// records PTIERR_VALUE_ERROR with newIndices left as the identity.
+// Lexi-order (renumber == 1) or BFS-like (renumber == 2, orderit.c's copy of
+// the same heap walk, :1030-1138).
 void orderit(ptiSparseTensor *tsr, ptiIndex **newIndices, int const renumber, ptiIndex const iterations)
 {
     ptiIndexRenumber(tsr, newIndices, renumber, iterations, 0, 1, 1);

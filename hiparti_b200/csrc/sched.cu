@@ -461,8 +461,17 @@ struct HiSmem {
 // thread group walks a contiguous slice: a lane decodes one nonzero's output
 // and operand rows from its block coordinates and offsets, the group shares
 // them by shuffles, gathers the operand rows and accumulates row runs.
+// Records in flight per thread group of the 3-D FP32 walk, and the CTAs per
+// SM the compiler is asked to fit (0: no register cap): compile-time choices.
+#ifndef PTI_HICOO_U
+#define PTI_HICOO_U 3
+#endif
+#ifndef PTI_HICOO_MINB
+#define PTI_HICOO_MINB 0
+#endif
+
 template <int G, int CPL, int U, class FT, int NIN>
-__global__ void __launch_bounds__(kSchedThreads) hicoo_sched_kernel(SchedArgs a)
+__global__ void __launch_bounds__(kSchedThreads, PTI_HICOO_MINB) hicoo_sched_kernel(SchedArgs a)
 {
     using L = HiSmem<NIN, CPL>;
     extern __shared__ __align__(128) unsigned char sm[];
@@ -943,7 +952,7 @@ template <int G, int CPL, class FT, int NIN>
 static int launch_hicoo(const SchedArgs &a, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = HiSmem<NIN, CPL>::total;
-    constexpr int U = NIN == 3 || CPL == 8 ? 2 : 3;  // nonzeros in flight per group
+    constexpr int U = NIN == 3 || CPL == 8 ? 2 : PTI_HICOO_U;  // nonzeros in flight per group
     auto k = hicoo_sched_kernel<G, CPL, U, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;

@@ -9,8 +9,12 @@ namespace pti {
 
 constexpr int kMaxModes = 8;
 
-// Nonzeros per tile of a per-mode HiCOO schedule (HicooModePlan::tile_block).
-constexpr int kPlanTile = 2048;
+// Nonzeros per tile of a per-mode HiCOO schedule (HicooModePlan::tile_block);
+// a power of two of at most 4096 (a compile-time choice, -DPTI_PLAN_TILE).
+#ifndef PTI_PLAN_TILE
+#define PTI_PLAN_TILE 2048
+#endif
+constexpr int kPlanTile = PTI_PLAN_TILE;
 
 // Per-mode schedule of a HiCOO tensor.  The blocks are re-ordered by their
 // block coordinate in the output mode (a materialised form of the reference's

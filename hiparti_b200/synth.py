@@ -187,3 +187,52 @@ def coords_torch(dims, nnz, seed, zipf_s=None, device="cuda"):
         cols.append((keys % d).to(torch.int32))
         keys = keys // d
     return cols[::-1]
+
+
+def sparse_lowrank_torch(dims, rank, support, noise=0.0, seed=0, device="cuda"):
+    """sparse_lowrank_tensor on a CUDA device with torch, for tens of millions
+    of nonzeros: component r has entries |N(0,1)| + 0.1 on `support` random
+    rows of every mode (zeros elsewhere) and weight U(1,10); the nonzeros are
+    the union of the components' support blocks (rank * support^N coordinates
+    before the rare overlaps merge), with values sum_r lambda_r prod_m
+    A_m[i_m, r] + N(0, noise^2).  Returns (inds as int32 tensors, FP32 values,
+    (lambda, factors) as FP64 tensors)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    dims = [int(d) for d in dims]
+    N = len(dims)
+    facs = [torch.zeros((d, rank), dtype=torch.float64, device=device) for d in dims]
+    keys = []
+    for r in range(rank):
+        rows = []
+        for m, d in enumerate(dims):
+            s = min(support, d)
+            idx = torch.randperm(d, generator=g, device=device)[:s]
+            facs[m][idx, r] = torch.randn(s, generator=g, device=device, dtype=torch.float64).abs_() + 0.1
+            rows.append(idx)
+        grid = torch.meshgrid(*rows, indexing="ij")
+        key = torch.zeros_like(grid[0].reshape(-1))
+        for gm, d in zip(grid, dims):
+            key = key * d + gm.reshape(-1)
+        keys.append(key)
+    keys = torch.unique(torch.cat(keys))
+    cols = []
+    k = keys.clone()
+    for d in reversed(dims):
+        cols.append(k % d)
+        k = k // d
+    cols = cols[::-1]
+    lam = torch.rand(rank, generator=g, device=device, dtype=torch.float64) * 9 + 1
+    vals = torch.zeros(keys.numel(), dtype=torch.float64, device=device)
+    step = 1 << 22
+    for z0 in range(0, keys.numel(), step):
+        model = lam.expand(min(step, keys.numel() - z0), rank).clone()
+        for a, c in zip(facs, cols):
+            model *= a[c[z0:z0 + step]]
+        vals[z0:z0 + step] = model.sum(1)
+    if noise:
+        vals += torch.randn(vals.numel(), generator=g, device=device, dtype=torch.float64) * noise
+    inds = [c.to(torch.int32) for c in cols]
+    return inds, vals.float(), (lam, facs)

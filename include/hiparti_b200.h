@@ -166,16 +166,23 @@ double SparseTensorFrobeniusNormSquared(ptiSparseTensor const * const ptien);
  * their order and their values are those of the reference's fscanf reader. */
 int  ptiLoadSparseTensor(ptiSparseTensor *tsr, ptiIndex start_index, char const * const fname);
 
-/* include/includes/sptensors.h:100 -- Lexi-order renumbering (renumber == 1)
- * on the GPU; newIndices[m][old] = new.  tsr is not modified.  sb_bits and tk
- * are unused; impl_num 0 or 1.  Other choices record PTIERR_VALUE_ERROR (see
- * ptiGetLastError) and leave the identity in newIndices. */
+/* include/includes/sptensors.h:100, src/sptensor/renumber.c:26-92;
+ * newIndices[m][old] = new.  tsr is not modified.  renumber == 1: Lexi-order
+ * on the GPU, `iterations` passes; impl_num 0, 1 or 2 (2 compares block
+ * indices before indices, which orders coordinates the same way).
+ * renumber == 2: BFS-like (renumber.c:534-839): the vertex lists are built on
+ * the GPU and the heap walk runs on the host; every vertex starts unvisited
+ * (the reference reads those marks uninitialised, renumber.c:768, so its own
+ * output varies from call to call).  sb_bits and tk are unused.  Other
+ * choices record PTIERR_VALUE_ERROR (see ptiGetLastError) and leave the
+ * identity in newIndices. */
 void ptiIndexRenumber(ptiSparseTensor * tsr, ptiIndex ** newIndices, int renumber, ptiIndex iterations,
                       ptiElementIndex sb_bits, int tk, int impl_num);
 /* include/includes/sptensors.h:101, src/sptensor/orderit.c:121-208 -- the same
- * Lexi-order.  (The reference's ptiIndexRenumber sorts the nonzeros with a
- * defective insertion sort and so depends on their order; both entry points
- * here give orderit's result.) */
+ * Lexi-order (renumber 1) or BFS-like (renumber 2).  (For impl_num 0 and 1 the
+ * reference's ptiIndexRenumber sorts the nonzeros with a defective insertion
+ * sort and so depends on their order; both entry points here give orderit's
+ * result.) */
 void orderit(ptiSparseTensor *tsr, ptiIndex **newIndices, int const renumber, ptiIndex const iterations);
 /* include/includes/sptensors.h:45 -- coordinates replaced by map_inds[m][old] */
 void ptiSparseTensorShuffleIndices(ptiSparseTensor *tsr, ptiIndex ** map_inds);
@@ -631,6 +638,19 @@ int ptiB200BatchCpdAls(ptiB200Batch *batch, ptiIndex niters, int precision, ptiI
                        float * const *dev_factors, float * const *dev_lambda, double *fits,
                        float *ms_per_iter, void *stream);
 void ptiB200BatchFree(ptiB200Batch *batch);
+
+/* Self-checks of the bounded device waits (no reference counterpart; they
+ * exercise the failure path without faulting or hanging the GPU).
+ * ptiB200BatchWaitProbe runs the batched ALS kernel on a one-task queue whose
+ * dependency nothing satisfies, with every wait bounded by wait_seconds (at
+ * most 2): the wait gives up and the call returns PTIERR_CUDA_ERROR, as a run
+ * whose queue stalled does; the batch stays usable (nothing it holds is
+ * written).  ptiB200MbarrierWaitProbe arms a shared-memory barrier for bytes
+ * that never arrive and waits `polls` polls: *gave_up = 1 when the bounded
+ * wait gave up, *completed = 1 when a second barrier, completed by its
+ * arrival alone, was seen complete. */
+int ptiB200BatchWaitProbe(ptiB200Batch *bt, double wait_seconds);
+int ptiB200MbarrierWaitProbe(unsigned polls, int *gave_up, int *completed);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -24,6 +24,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORC_SO = HERE / "_build" / "liborc.so"
 REF_SO = HERE / "_ref" / "libHiParTI.so"
+BFS_SO = HERE / "_ref" / "libbfsref.so"
 # the reference checkout: $HIPARTI_REF, else a "reference" directory beside the repository
 REF_SRC = Path(os.environ.get("HIPARTI_REF", HERE.parent.parent / "reference")).resolve()
 
@@ -180,6 +181,93 @@ class Orc:
                                           _ptr_array(inds, C.c_uint32), vals.ctypes.data_as(C.c_void_p),
                                           C.c_uint32(R), _ptr_array(mats, C.c_double),
                                           lam.ctypes.data_as(C.c_void_p))
+
+
+def bfs_like(dims, inds):
+    """BFS-like renumbering (src/sptensor/renumber.c:534-839; ptiIndexRenumber
+    with renumber == 2), restated with every vertex starting unvisited (the
+    reference reads the visit marks of other modes' vertices without setting
+    them, renumber.c:768).  The tensor is a hypergraph: a vertex per index of
+    every mode, a hyperedge per nonzero.  Mode by mode, the mode's vertices are
+    taken from a binary max-heap on a key, all keys 0 at first; the heap
+    compares the keys, and on equal keys prefers the smaller degree when it
+    sifts down (heapify, :666-701) and the larger degree when it sifts up
+    (heapIncreaseKey, :644-664).  The vertex taken gets the next new index;
+    every vertex of its hyperedges not yet visited in this mode's pass is
+    visited, and each hyperedge of that vertex raises by one the key of its
+    own vertex in the mode, if still in the heap.  Returns newIndices per
+    mode (old index -> new).  Pure Python: small tensors only."""
+    N = len(dims)
+    dims = [int(d) for d in dims]
+    inds = [np.asarray(i, np.int64) for i in inds]
+    nnz = inds[0].size if N else 0
+    lists = []
+    for m in range(N):
+        order = np.argsort(inds[m], kind="stable")
+        off = np.searchsorted(inds[m][order], np.arange(dims[m] + 1), side="left")
+        lists.append((order, off))
+    out = []
+    for d in range(N):
+        order_d, off_d = lists[d]
+        deg = np.diff(off_d)
+        n = dims[d]
+        heap = [0] + list(range(n))
+        pos = list(range(1, n + 1))  # pos[v]: heap slot of v, 0 once taken
+        key = [0] * n
+        size = n
+
+        def down(j):
+            while j <= size // 2:
+                l, r = 2 * j, 2 * j + 1
+                big = l if (key[heap[l]] > key[heap[j]] or
+                            (key[heap[l]] == key[heap[j]] and deg[heap[l]] < deg[heap[j]])) else j
+                if r <= size and (key[heap[r]] > key[heap[big]] or
+                                  (key[heap[r]] == key[heap[big]] and deg[heap[r]] < deg[heap[big]])):
+                    big = r
+                if big == j:
+                    break
+                heap[big], heap[j] = heap[j], heap[big]
+                pos[heap[big]], pos[heap[j]] = big, j
+                j = big
+
+        def up(v):
+            i = pos[v]
+            key[v] += 1
+            while i > 1 and (key[v] > key[heap[i >> 1]] or
+                             (key[v] == key[heap[i >> 1]] and deg[v] > deg[heap[i >> 1]])):
+                heap[i] = heap[i >> 1]
+                pos[heap[i]] = i
+                i >>= 1
+            heap[i] = v
+            pos[v] = i
+
+        for j in range(size // 2, 0, -1):
+            down(j)
+        visited = [np.zeros(dims[m], bool) for m in range(N)]
+        new = np.zeros(n, np.uint32)
+        for t in range(n):
+            v = heap[1]
+            heap[1] = heap[size]
+            pos[heap[1]] = 1
+            size -= 1
+            pos[v] = 0
+            down(1)
+            new[v] = t
+            for h in order_d[off_d[v]:off_d[v + 1]]:
+                for k in range(N):
+                    if k == d:
+                        continue
+                    w = inds[k][h]
+                    if visited[k][w]:
+                        continue
+                    visited[k][w] = True
+                    ok, oo = lists[k]
+                    for h2 in ok[oo[w]:oo[w + 1]]:
+                        u = inds[d][h2]
+                        if pos[u]:
+                            up(u)
+        out.append(new)
+    return out
 
 
 # ----------------------------------------------------------------------------
@@ -378,6 +466,24 @@ class Ref:
         vals = _np_from(out.values.values, n2 * st2, np.float32).reshape(n2, st2) if n2 else \
             np.empty((0, st2), np.float32)
         return finds, vals
+
+    @staticmethod
+    def bfs_available() -> bool:
+        return BFS_SO.exists()
+
+    def bfs_like(self, dims, inds, vals):
+        """The reference's ptiBFSLike (src/sptensor/renumber.c:794-839) from
+        oracle/_ref/libbfsref.so: its own source compiled with an allocator that
+        fills fresh blocks with 0xFF (oracle/ff_malloc.c), so the visit marks it
+        reads before writing are -1 ("not visited") and the result is
+        deterministic.  newIndices per mode."""
+        if not hasattr(self, "_bfs"):
+            self._bfs = C.CDLL(str(BFS_SO), mode=C.RTLD_LOCAL)
+        t, keep = self._coo(dims, inds, vals)
+        maps = [np.zeros(d, np.uint32) for d in dims]
+        arr = (C.c_void_p * len(dims))(*[m.ctypes.data for m in maps])
+        self._bfs.ptiBFSLike(C.byref(t), arr)
+        return maps
 
     def orderit(self, dims, inds, vals, iterations):
         """orderit(renumber=1) of the reference (src/sptensor/orderit.c:121-208),

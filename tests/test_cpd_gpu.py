@@ -93,3 +93,26 @@ def test_reference_entry_points_run(lib, cuda):
         res = coo.cpd_als(4, 3, variant=variant)
         assert [f.shape for f in res["factors"]] == [(d, 4) for d in dims]
         assert res["lambda_"].shape == (4,)
+
+
+def test_cpd_bf16_on_a_low_rank_million_nonzero_tensor(lib, cuda, orc):
+    """BF16 factors where the fit is far from 0: a 4-D tensor of exact CP rank
+    5 (each component on 22 rows of every mode, 1.17M nonzeros) plus
+    N(0, 0.05^2), R = 5, 30 iterations from one seeded start.  The FP64 oracle
+    reaches a fit near 0.99; the BF16 run with two closing FP32 sweeps must end
+    within 1e-4 of that fit with the same factors (factor match score >= 0.99,
+    Acar et al.: best column pairing, product of cosines times the weight
+    ratio)."""
+    from bench import factor_match_score
+    dims = (2000, 2000, 2000, 100)
+    inds, vals, _ = synth.sparse_lowrank_tensor(dims, 5, 22, noise=0.05, seed=21)
+    assert vals.size >= 1_000_000
+    R, iters = 5, 30
+    rng = np.random.default_rng(22)
+    init = [rng.random((d, R)).astype(np.float32) for d in dims]
+    o = orc.cpd_als(list(dims), inds, vals, R, iters, init)
+    assert o["fit"] > 0.9
+    for fmt in ("hicoo", "coo"):
+        lam, facs, fits = _device_cpd(dims, inds, vals, init, iters, fmt=fmt, precision="bf16", fp32_sweeps=2)
+        assert abs(fits[-1] - o["fit"]) < 1e-4, (fmt, fits[-1], o["fit"])
+        assert factor_match_score(lam, facs, o["lambda_"], o["factors"]) >= 0.99

@@ -64,3 +64,51 @@ def test_renumbering_gathers_planted_blocks(lib, cuda):
         t.free()
     assert nb1 == nblk  # one HiCOO block per planted block
     assert nb0 > 8 * nblk
+
+
+# ---------------------------------------------------------------------------
+# BFS-like (renumber == 2) and impl_num 2
+# ---------------------------------------------------------------------------
+def test_bfs_like_matches_golden_reference_vectors(lib, cuda):
+    from test_renumber import _bfs_cases
+    for dims, inds, vals, want in _bfs_cases():
+        got = COOTensor(dims, inds, vals).renumber(method="bfs")
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("dims,nnz,seed", [((300, 200, 100), 20000, 1), ((60, 50, 40, 30), 15000, 2),
+                                           ((5000, 40, 30), 12000, 3)])
+def test_bfs_like_matches_reference_and_oracle(lib, cuda, ref, dims, nnz, seed):
+    from oracle.oracle import Ref, bfs_like
+    from hiparti_b200 import synth
+    inds, vals = synth.zipf_tensor(dims, nnz, s=1.1, seed=seed)
+    got = COOTensor(dims, inds, vals).renumber(method="bfs")
+    again = COOTensor(dims, [i.copy() for i in inds], vals.copy()).renumber(method="bfs")
+    want = ref.bfs_like(list(dims), inds, vals) if Ref.bfs_available() else bfs_like(list(dims), inds)
+    for a, b, c in zip(got, again, want):
+        np.testing.assert_array_equal(a, b)  # deterministic
+        np.testing.assert_array_equal(a, c)
+        assert np.array_equal(np.sort(a), np.arange(a.size))
+
+
+def test_bfs_like_edge_cases(lib, cuda):
+    from oracle.oracle import bfs_like
+    # empty tensor, a mode of size one, indices without nonzeros
+    for dims, inds in [((4, 3, 2), [np.empty(0, np.uint32)] * 3),
+                       ((9, 1, 5), [np.array([0, 3, 3, 8], np.uint32), np.zeros(4, np.uint32),
+                                    np.array([4, 0, 2, 4], np.uint32)])]:
+        vals = np.ones(inds[0].size, np.float32)
+        got = COOTensor(dims, inds, vals).renumber(method="bfs")
+        for a, b in zip(got, bfs_like(list(dims), inds)):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("dims,nnz,its", CASES)
+def test_impl_num_2_matches_reference(lib, cuda, ref, dims, nnz, its):
+    inds, vals = random_tensor(dims, nnz, 0)
+    assert tie_free(dims, inds)
+    got = COOTensor(dims, inds, vals).renumber(its, impl_num=2)
+    want = ref.renumber(list(dims), inds, vals, its, impl_num=2)
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
