@@ -53,6 +53,8 @@ struct SchedArgs {
     float *out;
     uint32_t *err;
     const uint4 *bquad;         // HiCOO 4-D: per block {output, operand 0, 1, 2} block coordinates
+    const uint4 *recs;          // HiCOO: decoded records of the schedule (HicooModePlan::recs)
+    const float *rvals;         // HiCOO 4-D: their values
 };
 
 
@@ -302,8 +304,9 @@ __device__ __forceinline__ void process_records(const uint32_t *s_rec, uint32_t 
     if (owner) w.template merge<G>(a, s_slots, s_slot_row, s_slot_whole, g, lane, kGroups);
 }
 
-// Walks records [j0, j1) of a tile whose n records s_rec are in output-row
-// order and accumulates v * prod_k A_k[row_k] one row run at a time.  Every
+// Walks records [j0, j1) of a tile whose n records s_rec ({output row,
+// operand rows, value or third operand row}) are in output-row order and
+// accumulates v * prod_k A_k[row_k] one row run at a time.  Every
 // record is walkable: the decode gave a record with a bad coordinate value 0
 // and operand offsets 0, and an output row kNoRow only where its own row is
 // out of range (such records sort after every valid row), so the rows of a
@@ -339,6 +342,7 @@ __device__ __forceinline__ void walk_rows(const uint4 *s_rec, const float *s_v3,
     const FT *base[NIN];
 #pragma unroll
     for (int k = 0; k < NIN; ++k) base[k] = static_cast<const FT *>(a.in_mat[k]) + (active ? col : 0u);
+    const uint32_t stride = a.stride;
     float acc[CPL];
 #pragma unroll
     for (int c = 0; c < CPL; ++c) acc[c] = 0.f;
@@ -375,7 +379,7 @@ __device__ __forceinline__ void walk_rows(const uint4 *s_rec, const float *s_v3,
             r[u] = s_rec[j + u];
             const uint32_t rr[3] = {r[u].y, r[u].z, r[u].w};
 #pragma unroll
-            for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + rr[k], 0);
+            for (int k = 0; k < NIN; ++k) f[u][k].load(base[k] + (size_t)rr[k] * stride, 0);
         }
         if (__all_sync(__activemask(), r[U - 1].x == cur)) {
 #pragma unroll
@@ -396,7 +400,7 @@ __device__ __forceinline__ void walk_rows(const uint4 *s_rec, const float *s_v3,
         const uint32_t rr[3] = {r.y, r.z, r.w};
         RowPart<CPL, FT> f[NIN];
 #pragma unroll
-        for (int k = 0; k < NIN; ++k) f[k].load(base[k] + rr[k], 0);
+        for (int k = 0; k < NIN; ++k) f[k].load(base[k] + (size_t)rr[k] * stride, 0);
         if (r.x != cur) {
             end_run();
             cur = r.x;
@@ -464,7 +468,7 @@ struct HiSmem {
 // Records in flight per thread group of the 3-D FP32 walk, and the CTAs per
 // SM the compiler is asked to fit (0: no register cap): compile-time choices.
 #ifndef PTI_HICOO_U
-#define PTI_HICOO_U 3
+#define PTI_HICOO_U 2
 #endif
 #ifndef PTI_HICOO_MINB
 #define PTI_HICOO_MINB 0
@@ -577,9 +581,8 @@ __global__ void __launch_bounds__(kSchedThreads, PTI_HICOO_MINB) hicoo_sched_ker
                     ok_in = ok_in && rk < a.in_dim[k];
                     r[k] = (uint32_t)rk;
                 }
-                // operand rows become element offsets (below 2^32: schedule_supported)
 #pragma unroll
-                for (int k = 0; k < NIN; ++k) r[k] = ok_in ? r[k] * a.stride : 0u;
+                for (int k = 0; k < NIN; ++k) r[k] = ok_in ? r[k] : 0u;
                 vv[p] = ok_o && ok_in ? s_val[z] : 0.f;
                 if (NIN == 1) r[1] = __float_as_uint(vv[p]);
                 if (NIN == 2) r[2] = __float_as_uint(vv[p]);
@@ -609,6 +612,106 @@ __global__ void __launch_bounds__(kSchedThreads, PTI_HICOO_MINB) hicoo_sched_ker
     const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;
     const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
     walk_rows<G, CPL, U, FT, NIN>(s_rec, s_v3, n, j0, j1, g, lane, a, s_slots, s_slot_row, s_slot_whole);
+}
+
+template <int NIN, int CPL>
+struct RecSmem {
+    // byte offsets inside the dynamic shared memory of hicoo_rec_kernel
+    static constexpr uint32_t rec = 0;                                 // uint4[kHiTile]
+    static constexpr uint32_t rval = rec + 16 * kHiTile;               // float[kHiTile] (4-D only)
+    static constexpr uint32_t slots = rval + (NIN == 3 ? 4 * kHiTile : 0);  // float[kSchedThreads * CPL]
+    static constexpr uint32_t total = slots + 4 * kSchedThreads * CPL;
+};
+
+// HiCOO schedule, one CTA per tile of kHiTile nonzeros whose records the
+// schedule already holds decoded (HicooModePlan::recs, in output-row order
+// within the tile): one bulk copy stages them (and the 4-D values), then the
+// thread groups walk contiguous slices (walk_rows).
+template <int G, int CPL, int U, class FT, int NIN>
+__global__ void __launch_bounds__(kSchedThreads, PTI_HICOO_MINB) hicoo_rec_kernel(SchedArgs a)
+{
+    using L = RecSmem<NIN, CPL>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t s_slot_row[kSchedThreads];
+    __shared__ uint8_t s_slot_whole[kSchedThreads];
+    uint4 *s_rec = reinterpret_cast<uint4 *>(sm + L::rec);
+    float *s_v3 = reinterpret_cast<float *>(sm + L::rval);
+    float *s_slots = reinterpret_cast<float *>(sm + L::slots);
+    const uint32_t tid = threadIdx.x;
+    const uint64_t z0 = (uint64_t)blockIdx.x * kHiTile;
+    const uint32_t n = (uint32_t)((a.nnz - z0) < (uint64_t)kHiTile ? (a.nnz - z0) : (uint64_t)kHiTile);
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bv = NIN == 3 ? round16(4 * n) : 0u;
+        mbar_arrive_expect_tx(&mbar, 16 * n + bv);
+        bulk_g2s_ef(s_rec, a.recs + z0, 16 * n, &mbar);
+        if constexpr (NIN == 3) bulk_g2s_ef(s_v3, a.rvals + z0, bv, &mbar);
+    }
+    const bool ok = mbar_wait_bounded(&mbar, 0);
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) {
+            atomicOr(a.err, 2u);
+            mbar_wait_bounded(&mbar, 0);
+        }
+        return;
+    }
+    const uint32_t g = tid / G, lane = tid % G;
+    constexpr uint32_t kGroups = kSchedThreads / G;
+    // an odd slice length puts the groups' first records on different shared-memory banks
+    const uint32_t per = ((n + kGroups - 1) / kGroups) | 1u;
+    const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
+    walk_rows<G, CPL, U, FT, NIN>(s_rec, s_v3, n, j0, j1, g, lane, a, s_slots, s_slot_row, s_slot_whole);
+}
+
+// Decodes a HiCOO schedule into records (HicooModePlan::recs): the nonzero at
+// schedule position j lies in block tile_block[j / kHiTile] + lblk[j] of the
+// schedule's block order.  Operands in increasing mode order.
+struct RecBuildArgs {
+    uint64_t n, nb;
+    uint32_t nin, sb;
+    const uint16_t *lblk;
+    const uint32_t *tile_block;
+    const uint32_t *out_bind;
+    const uint8_t *out_eind;
+    uint32_t out_dim;
+    const uint32_t *in_bind[3];
+    const uint8_t *in_eind[3];
+    uint32_t in_dim[3];
+    const float *vals;
+    uint4 *recs;
+    float *rvals;
+    uint32_t *err;
+};
+
+__global__ void build_records_kernel(RecBuildArgs r)
+{
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < r.n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b0 = (uint64_t)r.tile_block[j / kHiTile] + r.lblk[j];
+        const bool ok_b = b0 < r.nb;
+        const uint64_t b = ok_b ? b0 : 0;
+        const uint64_t o = ((uint64_t)r.out_bind[b] << r.sb) + r.out_eind[j];
+        const bool ok_o = ok_b && o < r.out_dim;
+        uint32_t row[3] = {0u, 0u, 0u};
+        bool ok_in = true;
+        for (uint32_t k = 0; k < r.nin; ++k) {
+            const uint64_t rk = ((uint64_t)r.in_bind[k][b] << r.sb) + r.in_eind[k][j];
+            ok_in = ok_in && rk < r.in_dim[k];
+            row[k] = (uint32_t)rk;
+        }
+        if (!ok_in) row[0] = row[1] = row[2] = 0u;
+        const float v = ok_o && ok_in ? r.vals[j] : 0.f;
+        uint4 rec = make_uint4(ok_o ? (uint32_t)o : kNoRow, row[0], row[1], row[2]);
+        if (r.nin == 1) rec.z = __float_as_uint(v);
+        if (r.nin == 2) rec.w = __float_as_uint(v);
+        if (r.nin == 3) r.rvals[j] = v;
+        r.recs[j] = rec;
+        if (!(ok_o && ok_in)) atomicOr(r.err, 1u);
+    }
 }
 
 // COO schedule: packed records sorted by output index; no sorting in the kernel.
@@ -926,6 +1029,32 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals
                                                          P.binds[o[1]].as<uint32_t>(), P.binds[o[2]].as<uint32_t>(),
                                                          nb, P.bquad.as<uint4>());
         }
+        // 5. the decoded records the MTTKRP kernel stages
+        PTI_TRY(ensure_err_word(t, s));
+        PTI_CUDA(P.recs.alloc(padded(n * 16), s), mod);
+        if (N == 4) PTI_CUDA(P.rvals.alloc(padded(n * 4), s), mod);
+        RecBuildArgs ra{};
+        ra.n = n;
+        ra.nb = nb;
+        ra.nin = N - 1;
+        ra.sb = t->sb;
+        ra.lblk = P.lblk.as<uint16_t>();
+        ra.tile_block = P.tile_block.as<uint32_t>();
+        ra.out_bind = P.binds[mode].as<uint32_t>();
+        ra.out_eind = P.einds[mode].as<uint8_t>();
+        ra.out_dim = t->ndims[mode];
+        for (uint32_t k = 0, i = 0; k < N; ++k)
+            if (k != mode) {
+                ra.in_bind[i] = P.binds[k].as<uint32_t>();
+                ra.in_eind[i] = P.einds[k].as<uint8_t>();
+                ra.in_dim[i] = t->ndims[k];
+                ++i;
+            }
+        ra.vals = P.vals.as<float>();
+        ra.recs = P.recs.as<uint4>();
+        ra.rvals = N == 4 ? P.rvals.as<float>() : nullptr;
+        ra.err = err_word(t);
+        build_records_kernel<<<grid_n(n), 256, 0, s>>>(ra);
     }
     inv.reset();
     PTI_CUDA(cudaGetLastError(), mod);
@@ -936,24 +1065,66 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals
 // ---------------------------------------------------------------------------
 // Launch
 // ---------------------------------------------------------------------------
+// Records in flight per group of the COO walk (FP32, R <= 32) and the CTAs
+// per SM its register budget is set for: compile-time choices.
+#ifndef PTI_COO_U
+#define PTI_COO_U 3
+#endif
+#ifndef PTI_COO_MINB
+#define PTI_COO_MINB 4
+#endif
+
 template <int G, int CPL, int U, class FT, int NIN>
 static int launch_coo(const SchedArgs &a, const uint32_t *recs, unsigned ntiles, cudaStream_t s)
 {
     const size_t smem = (size_t)kTile * Rec<NIN>::words * 4 + (size_t)kSchedThreads * CPL * 4;
     constexpr int UU = NIN == 3 && U > 2 ? 2 : U;  // 4-D records hold more registers per nonzero
-    auto k = coo_sched_kernel<G, CPL, UU, 4, FT, NIN>;
+    auto k = coo_sched_kernel<G, CPL, UU, PTI_COO_MINB, FT, NIN>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a, recs);
     return 0;
 }
 
+// Which HiCOO kernel runs (a compile-time choice): 0 decodes every tile from
+// the staged HiCOO arrays (hicoo_sched_kernel), 2 stages the schedule's
+// decoded records (hicoo_rec_kernel), 1 takes the records for 4-D tensors and
+// for BF16 factors and decodes 3-D FP32 tiles.
+#ifndef PTI_REC_POLICY
+#define PTI_REC_POLICY 1
+#endif
+// CTAs per SM the BF16 record kernels are held to (0: no limit).  Their walk
+// is bound by the L1 data pipe and feeds on the L1 that a further CTA's
+// shared memory would take.
+#ifndef PTI_REC_BF16_CTAS
+#define PTI_REC_BF16_CTAS 3
+#endif
+
+template <class FT, int NIN>
+constexpr bool use_records()
+{
+    return PTI_REC_POLICY == 2 || (PTI_REC_POLICY == 1 && (NIN == 3 || sizeof(FT) == 2));
+}
+
 template <int G, int CPL, class FT, int NIN>
 static int launch_hicoo(const SchedArgs &a, unsigned ntiles, cudaStream_t s)
 {
-    const size_t smem = HiSmem<NIN, CPL>::total;
     constexpr int U = NIN == 3 || CPL == 8 ? 2 : PTI_HICOO_U;  // nonzeros in flight per group
-    auto k = hicoo_sched_kernel<G, CPL, U, FT, NIN>;
+    size_t smem;
+    void (*k)(SchedArgs);
+    if constexpr (use_records<FT, NIN>()) {
+        smem = RecSmem<NIN, CPL>::total;
+        if (sizeof(FT) == 2 && PTI_REC_BF16_CTAS > 0) {
+            // more dynamic shared memory than 1/(n+1) of the SM's 228 KB (with
+            // the static part and the 1 KB the runtime keeps per CTA)
+            const size_t cap = 233472 / (PTI_REC_BF16_CTAS + 1) - 1408 - 1024 + 16;
+            smem = smem > cap ? smem : cap;
+        }
+        k = hicoo_rec_kernel<G, CPL, U, FT, NIN>;
+    } else {
+        smem = HiSmem<NIN, CPL>::total;
+        k = hicoo_sched_kernel<G, CPL, U, FT, NIN>;
+    }
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PTIERR_CUDA_ERROR;
     k<<<ntiles, kSchedThreads, smem, s>>>(a);
@@ -991,10 +1162,10 @@ static int launch_r(bool hicoo, bool wide, const SchedArgs &a, const uint32_t *r
         if (R <= 64) return launch_hicoo<16, 4, FT, NIN>(a, ntiles, s);
         return launch_hicoo<32, 4, FT, NIN>(a, ntiles, s);
     }
-    if (R <= 4) return launch_coo<1, 4, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 8) return launch_coo<2, 4, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 16) return launch_coo<4, 4, 3, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 32) return launch_coo<8, 4, 3, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 4) return launch_coo<1, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 8) return launch_coo<2, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 16) return launch_coo<4, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 32) return launch_coo<8, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
     if (R <= 64) return launch_coo<16, 4, 2, FT, NIN>(a, recs, ntiles, s);
     return launch_coo<32, 4, 2, FT, NIN>(a, recs, ntiles, s);
 }
@@ -1047,21 +1218,22 @@ int mttkrp_scheduled(ptiB200Tensor *t, const void *const *mats, int ft, uint32_t
         a.tile_block = P.tile_block.as<uint32_t>();
         a.out_bind = P.binds[mode].as<uint32_t>();
         a.out_eind = P.einds[mode].as<uint8_t>();
-        // 4-D: the operands in increasing mode order, the order of the block
-        // records (the product's order only changes FP32 rounding)
-        for (uint32_t i = 1, c = 0; i < N; ++i) {
-            uint32_t k = mats_order[i];
-            if (N == 4) {
-                while (c == mode) ++c;
-                k = c++;
+        // the operands in increasing mode order: the order of the decoded
+        // records and of the 4-D block records (a product of two factors does
+        // not depend on the order, of three only in its FP32 rounding)
+        (void)mats_order;
+        for (uint32_t i = 0, k = 0; k < N; ++k)
+            if (k != mode) {
+                a.in_bind[i] = P.binds[k].as<uint32_t>();
+                a.in_eind[i] = P.einds[k].as<uint8_t>();
+                a.in_dim[i] = t->ndims[k];
+                a.in_mat[i] = mats[k];
+                ++i;
             }
-            a.in_bind[i - 1] = P.binds[k].as<uint32_t>();
-            a.in_eind[i - 1] = P.einds[k].as<uint8_t>();
-            a.in_dim[i - 1] = t->ndims[k];
-            a.in_mat[i - 1] = mats[k];
-        }
         a.bquad = N == 4 ? P.bquad.as<uint4>() : nullptr;
         a.vals = P.vals.as<float>();
+        a.recs = P.recs.as<uint4>();
+        a.rvals = P.rvals.as<float>();
     } else {
         // records hold the operand modes in increasing order
         ntiles = (unsigned)((t->nnz + kTile - 1) / kTile);

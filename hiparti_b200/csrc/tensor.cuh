@@ -35,6 +35,13 @@ struct HicooModePlan {
     DevBuf tile_block;                    // uint32 [ntiles+1]: first block of each tile
     uint32_t ntiles = 0;
     DevBuf bquad;                         // 4-D: uint4 [nb], {output, operands in increasing mode order}
+    // The same nonzeros decoded, in schedule order: {output row, operand
+    // rows in increasing mode order, value bits (3-D) or the third operand
+    // row (4-D)}, with the 4-D values beside them.  A coordinate out of range
+    // decodes to a record that adds nothing (value 0, operand rows 0; output
+    // row kNoRow when the output coordinate is the bad one).
+    DevBuf recs;                          // uint4 [nnz]
+    DevBuf rvals;                         // float [nnz], 4-D only
 };
 
 // Per-mode schedule of a COO tensor: nonzeros sorted by the output-mode index,
