@@ -1,24 +1,32 @@
 // probe.cu -- the L2 read bandwidth of this GPU, measured by a kernel of this
 // library: the ceiling against which the MTTKRP's factor-row gathers (2 rows
 // of R values per nonzero for a 3-D tensor, served from L1 and L2) are read.
-// A buffer well inside L2 is streamed with 16-byte loads; the first pass
-// brings it into L2 and is not timed.
+// A buffer inside L2 is streamed with 16-byte loads; the first pass brings
+// it into L2 and is not timed.  Each thread needs several loads per pass for
+// all eight to be in flight: on B200 buffers of 64-96 MiB read at the same
+// rate (18.8 TB/s), 16 MiB (under four loads per thread) at half of it.
 #include "common.cuh"
 
 namespace pti {
 namespace {
 
+constexpr int kProbeLoads = 8;  // independent 16-byte loads in flight per thread
+
+// Every thread issues kProbeLoads independent 16-byte L2-only loads (__ldcg:
+// ld.global.cg, no L1 allocation) before it uses any of them, so the figure
+// is the L2's read rate rather than the latency of one load per thread.
 __global__ void l2_read_kernel(const uint4 *buf, uint64_t n16, unsigned reps, uint32_t *sink)
 {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint32_t acc = 0;
     for (unsigned r = 0; r < reps; ++r)
-        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x) {
-            uint4 v;
-            // L2 only (.cg: the loads do not allocate in L1)
-            asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];"
-                         : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                         : "l"(buf + i));
-            acc ^= v.x ^ v.y ^ v.z ^ v.w;
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += kProbeLoads * stride) {
+            uint4 v[kProbeLoads];
+#pragma unroll
+            for (int k = 0; k < kProbeLoads; ++k)
+                v[k] = i + k * stride < n16 ? __ldcg(buf + i + k * stride) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int k = 0; k < kProbeLoads; ++k) acc ^= v[k].x ^ v[k].y ^ v[k].z ^ v[k].w;
         }
     if (acc == 0x9e3779b9u) sink[0] = acc;  // keeps the loads; practically never written
 }

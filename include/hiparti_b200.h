@@ -654,9 +654,10 @@ int ptiB200MbarrierWaitProbe(unsigned polls, int *gave_up, int *completed);
 
 /* The L2 read bandwidth of the current GPU (no reference counterpart): a
  * kernel of this library streams a buffer of `bytes` (1 MiB to 1 GiB; choose
- * one well inside L2) with 16-byte L2-only loads `reps` times after one
- * untimed pass; *gbps receives bytes * reps / time.  The bench reads the
- * MTTKRP's factor-row gathers against it. */
+ * one inside L2 and large enough for eight loads per thread, e.g. 64 MiB on
+ * B200) with 16-byte L2-only loads `reps` times after one untimed pass;
+ * *gbps receives bytes * reps / time.  The bench reads the MTTKRP's
+ * factor-row gathers against it. */
 int ptiB200ProbeL2ReadBandwidth(unsigned long long bytes, unsigned reps, double *gbps);
 
 #if defined(__GNUC__)
