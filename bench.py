@@ -824,6 +824,21 @@ def run_batched(args):
     return out
 
 
+def pool_used_bytes():
+    """Bytes in use in the current device's default memory pool (the pool the
+    library's cudaMallocAsync draws from), or None where it cannot be read."""
+    import torch
+    try:
+        from cuda.bindings import driver as drv
+        err, pool = drv.cuDeviceGetDefaultMemPool(torch.cuda.current_device())
+        if err != drv.CUresult.CUDA_SUCCESS:
+            return None
+        err, v = drv.cuMemPoolGetAttribute(pool, drv.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+        return int(v) if err == drv.CUresult.CUDA_SUCCESS else None
+    except Exception:
+        return None
+
+
 def run_ours_mttkrp(args, rank, world):
     import torch
     from hiparti_b200 import HiCOOTensor, ffi, lib
@@ -836,10 +851,15 @@ def run_ours_mttkrp(args, rank, world):
     N = 3
     # per-mode schedules (built once per tensor, reused by every MTTKRP)
     torch.cuda.synchronize()
+    used_before = pool_used_bytes()
     t0 = time.perf_counter()
     h.prepare()
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
+    used_after = pool_used_bytes()
+    # device memory the three schedules hold (the library allocates from the
+    # device's default memory pool; freed temporaries do not count)
+    schedule_bytes = used_after - used_before if used_before is not None and used_after is not None else None
     outs = [torch.empty((d, stride), dtype=torch.float32, device=dev) for d in C2_DIMS]
     bytes_mode = [hicoo_bytes(nnz, nb, C2_DIMS, C2_R, N) for _ in range(N)]
     step_bytes = sum(bytes_mode)
@@ -910,7 +930,8 @@ def run_ours_mttkrp(args, rank, world):
         "data": "synthetic (seeded Zipf(1.1) coordinates, U(0,1) values and factors)",
         "config": {"workload": f"C2 HiCOO MTTKRP, 3-D 200000x150000x20000, {nnz // 1000000}M nnz Zipf(1.1), "
                                "R=32, sb=7 sk=10 sc=14, FP32, all 3 modes per step",
-                   "nnz": nnz, "nb": nb, "prepare_s": round(prep_s, 3), "rank": C2_R, "modes_per_step": N,
+                   "nnz": nnz, "nb": nb, "prepare_s": round(prep_s, 3), "schedule_device_bytes": schedule_bytes,
+                   "rank": C2_R, "modes_per_step": N,
                    "algorithmic_bytes_per_step": step_bytes,
                    "l2": "inputs larger than L2 (tensor 0.8 GB vs 126 MB L2)",
                    "parallelism": f"replicas x{world}", "conversion_s": round(conv_s, 3),
