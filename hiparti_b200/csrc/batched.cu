@@ -626,15 +626,16 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
     __shared__ uint64_t mbar;
     __shared__ uint32_t s_q;
     __shared__ int s_ok;
+    __shared__ int s_copies_ok;  // 0 once a tile's bulk copies missed their wait bound
     const uint32_t tid = threadIdx.x;
     const uint32_t it = *a.iter;
     uint32_t *head = a.ctrl, *tiles_done = a.ctrl + 1, *dense_done = a.ctrl + 1 + 3 * a.ntensors;
     if (tid == 0) {
         mbar_init(&mbar, 1);
         mbar_fence_init();
+        s_copies_ok = 1;
     }
     uint32_t phase = 0;
-    bool copies_ok = true;  // false once a tile's bulk copies missed their wait bound
     __syncthreads();
     for (;;) {
         if (tid == 0) s_q = atomicAdd(head, 1u);
@@ -654,7 +655,8 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_als_kernel(BatchArgs a)
         __syncthreads();
         if (s_ok) {
             if (dense) dense_task(a.tens + b, b, m, it, a, sm, sizeof(FT) == 2);
-            else if (copies_ok) copies_ok = tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err);
+            else if (s_copies_ok && !tile_task<CPL, FT>(a.plans + pid, task.y, sm, &mbar, phase, a.err) && tid == 0)
+                s_copies_ok = 0;  // read by the next task after the barrier below
         }
         // shared memory written by this task may next be filled by bulk copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
