@@ -1,6 +1,6 @@
 // tma.cuh -- 1-D bulk copies (cp.async.bulk, the TMA engine) into shared
 // memory with an mbarrier, plus bounded waits.  Used only on this GPU's own
-// memory and without cluster multicast.
+// memory, each copy into the issuing CTA's own shared memory.
 #pragma once
 #include <cstdint>
 
