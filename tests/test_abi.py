@@ -111,3 +111,12 @@ def test_hicoo_struct_round_trip(lib):
                     [np.array([0, 1], np.uint8)] * 3, np.array([1, 2], np.float32))
     assert h.nb == 1 and h.nnz == 2
     assert h.c.bptr.len == 2 and h.c.binds[0].data[0] == 1
+
+
+def test_l2_probe_rejects_bad_arguments_before_any_gpu_work(lib):
+    gb = ffi.new("double *", -1.0)
+    assert lib.ptiB200ProbeL2ReadBandwidth(1 << 19, 10, gb) == 3      # under 1 MiB: PTIERR_VALUE_ERROR
+    assert lib.ptiB200ProbeL2ReadBandwidth(64 << 20, 0, gb) == 3      # no repetition
+    assert lib.ptiB200ProbeL2ReadBandwidth(2 << 30, 10, gb) == 3      # over 1 GiB
+    assert lib.ptiB200ProbeL2ReadBandwidth(64 << 20, 10, ffi.NULL) == 3
+    assert gb[0] == -1.0
