@@ -171,6 +171,35 @@ def test_device_api_torch(lib, cuda, orc, fmt, dtype):
     dt.free()
 
 
+@pytest.mark.parametrize("N", [3, 4])
+@pytest.mark.parametrize("dtype", ["float32", "bfloat16"])
+@pytest.mark.parametrize("R", [1, 3, 8, 16, 24, 32, 40, 64, 100, 128, 129, 200])
+def test_scheduled_hicoo_ranks(lib, cuda, orc, N, dtype, R):
+    """Every lane-group shape of the scheduled HiCOO walks: the in-kernel
+    decode (3-D, FP32 factors) and the pre-decoded records (4-D, and BF16
+    factors) from 1 lane per nonzero up to 32, both BF16 row widths, and the
+    direct kernel above R = 128; the BF16 case against the oracle on the
+    same BF16-rounded factors."""
+    import torch
+    dims = (300, 200, 100) if N == 3 else (120, 90, 60, 40)
+    inds, vals = synth.zipf_tensor(dims, 30000, s=1.1, seed=R + N)
+    mats = synth.factor_matrices(dims, R, seed=R + 1)
+    tdt = getattr(torch, dtype)
+    dmats = [torch.from_numpy(m).to(cuda).to(tdt) for m in mats]
+    ref_mats = [d.float().cpu().numpy() for d in dmats]
+    h = orc.hicoo_build(dims, inds, vals, 5, 7, 9)
+    dt = DeviceTensor.from_hicoo(HiCOOTensor(dims, 5, 7, 9, h["bptr"], h["binds"], h["einds"], h["vals"]))
+    for m in range(N):
+        out = dt.mttkrp(dmats, m, rank=R)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        ref = orc.mttkrp_coo(inds, vals, ref_mats, R, m)[: dims[m]]
+        assert rel_err(got[:, :R], ref[:, :R]) < TOL, (m, R)
+        assert np.all(got[:, R:] == 0)
+    dt.check()
+    dt.free()
+
+
 @pytest.mark.parametrize("R", [10, 32])
 def test_rank_matrix_entry_points_match_reference(lib, cuda, ref, R):
     """ptiMTTKRPHiCOO_MatrixTiling and the OpenMP MatrixTiling variants
