@@ -18,37 +18,76 @@ struct KVArgs {
 };
 
 // A group of G lanes per nonzero; each lane multiplies 4 columns across the
-// modes and the group sums its lanes with shuffles.
-template <int G>
+// modes and the group sums its lanes with shuffles.  A warp takes 32/G * U
+// consecutive nonzeros per pass: their coordinates are read once, coalesced,
+// by one lane each and handed to the groups with shuffles, and each group
+// then has the rows of U nonzeros in flight.
+template <int G, int U, int NM>
 __global__ void __launch_bounds__(256) kruskal_values_kernel(KVArgs a)
 {
     constexpr uint32_t kGroupsPerWarp = 32 / G;
-    const uint32_t lane = threadIdx.x % G;
+    constexpr uint32_t kPer = kGroupsPerWarp * U;  // nonzeros per warp and pass (<= 32)
+    static_assert(kPer <= 32, "one coordinate per lane");
+    const uint32_t lane32 = threadIdx.x % 32, lane = lane32 % G, grp = lane32 / G;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) / 32;
     // the loop bound is uniform across a warp, so every lane reaches the shuffles
-    for (uint64_t base = warp * kGroupsPerWarp; base < a.nnz; base += nwarps * kGroupsPerWarp) {
-        const uint64_t z = base + (threadIdx.x % 32) / G;
-        const bool live = z < a.nnz;
-        float s = 0.f;
-        if (live) {
-            uint32_t rows[kMaxModes];
+    for (uint64_t base = warp * kPer; base < a.nnz; base += nwarps * kPer) {
+        uint32_t rows[U][NM];
+        const uint64_t zt = base + lane32;
+        const bool have = lane32 < kPer && zt < a.nnz;
+        uint32_t mine[NM];
 #pragma unroll
-            for (int k = 0; k < kMaxModes; ++k)
-                if (k < (int)a.nmodes) rows[k] = __ldg(a.inds[k] + z);
-            for (uint32_t col = lane * 4; col < a.R; col += 4 * G) {
-                float4 p = load4(a.mats[0] + (size_t)rows[0] * a.stride, col);
+        for (int k = 0; k < NM; ++k) mine[k] = have && k < (int)a.nmodes ? __ldg(a.inds[k] + zt) : 0u;
 #pragma unroll
-                for (int k = 1; k < kMaxModes; ++k)
-                    if (k < (int)a.nmodes) p = mul4(p, load4(a.mats[k] + (size_t)rows[k] * a.stride, col));
-                p = mask4(p, col, a.R);
-                s += (p.x + p.y) + (p.z + p.w);
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < NM; ++k)
+                rows[u][k] = k < (int)a.nmodes ? __shfl_sync(0xffffffffu, mine[k], grp * U + u) : 0u;
+        float s[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) s[u] = 0.f;
+        for (uint32_t col = lane * 4; col < a.R; col += 4 * G) {
+            float4 p[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) p[u] = load4(a.mats[0] + (size_t)rows[u][0] * a.stride, col);
+#pragma unroll
+            for (int k = 1; k < NM; ++k)
+                if (k < (int)a.nmodes) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        p[u] = mul4(p[u], load4(a.mats[k] + (size_t)rows[u][k] * a.stride, col));
+                }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                p[u] = mask4(p[u], col, a.R);
+                s[u] += (p[u].x + p[u].y) + (p[u].z + p[u].w);
             }
         }
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
-        if (live && lane == 0) a.out[z] = s;
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o, G);
+        if (lane == 0) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t z = base + grp * U + u;
+                if (z < a.nnz) a.out[z] = s[u];
+            }
+        }
     }
+}
+
+#ifndef PTI_KV_U
+#define PTI_KV_U 2
+#endif
+// nonzeros in flight per group (32/G * U <= 32): on a 3-D tensor of 20M
+// nonzeros at R = 64, 2 gave the fastest gradient (4 costs more registers
+// than its extra rows in flight return)
+template <int G>
+constexpr int kv_u()
+{
+    return G < PTI_KV_U ? G : PTI_KV_U;
 }
 
 static int lanes_for(uint32_t R)
@@ -57,6 +96,21 @@ static int lanes_for(uint32_t R)
     int g = 1;
     while ((uint32_t)g < q && g < 32) g *= 2;
     return g;
+}
+
+template <int NM>
+static int launch_kv(int G, const KVArgs &a, unsigned grid, cudaStream_t s)
+{
+    constexpr bool any = NM == kMaxModes;  // any order: one nonzero in flight per group
+    switch (G) {
+        case 1: kruskal_values_kernel<1, any ? 1 : kv_u<1>(), NM><<<grid, 256, 0, s>>>(a); break;
+        case 2: kruskal_values_kernel<2, any ? 1 : kv_u<2>(), NM><<<grid, 256, 0, s>>>(a); break;
+        case 4: kruskal_values_kernel<4, any ? 1 : kv_u<4>(), NM><<<grid, 256, 0, s>>>(a); break;
+        case 8: kruskal_values_kernel<8, any ? 1 : kv_u<8>(), NM><<<grid, 256, 0, s>>>(a); break;
+        case 16: kruskal_values_kernel<16, any ? 1 : kv_u<16>(), NM><<<grid, 256, 0, s>>>(a); break;
+        default: kruskal_values_kernel<32, any ? 1 : kv_u<32>(), NM><<<grid, 256, 0, s>>>(a); break;
+    }
+    return 0;
 }
 
 }  // namespace pti
@@ -90,13 +144,13 @@ int ptiB200KruskalValues(ptiB200Tensor *t, const float *const *dev_factors, ptiI
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((t->nnz * G + 255) / 256, (uint64_t)sm_count() * 16));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    switch (G) {
-        case 1: kruskal_values_kernel<1><<<grid, 256, 0, s>>>(a); break;
-        case 2: kruskal_values_kernel<2><<<grid, 256, 0, s>>>(a); break;
-        case 4: kruskal_values_kernel<4><<<grid, 256, 0, s>>>(a); break;
-        case 8: kruskal_values_kernel<8><<<grid, 256, 0, s>>>(a); break;
-        case 16: kruskal_values_kernel<16><<<grid, 256, 0, s>>>(a); break;
-        default: kruskal_values_kernel<32><<<grid, 256, 0, s>>>(a); break;
+    // 3- and 4-mode tensors: U nonzeros in flight per group; other orders one
+    if (t->nmodes == 3) {
+        PTI_TRY(launch_kv<3>(G, a, grid, s));
+    } else if (t->nmodes == 4) {
+        PTI_TRY(launch_kv<4>(G, a, grid, s));
+    } else {
+        PTI_TRY(launch_kv<kMaxModes>(G, a, grid, s));
     }
     PTI_CUDA(cudaGetLastError(), mod);
     return 0;

@@ -91,3 +91,32 @@ def test_gradient_at_scale_vs_oracle(lib, cuda, orc):
         want = orc.mttkrp_coo(inds, resid, facs, R, k)[: dims[k]]
         assert rel_err(tf[k].grad.detach().cpu().numpy(), want) < 1e-5
     dt.free()
+
+
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
+@pytest.mark.parametrize("R", [1, 3, 8, 17, 33, 64, 100, 128, 200])
+def test_kruskal_values_every_group_shape(lib, cuda, N, R):
+    """The CP model at the nonzeros for every lane-group shape (1 to 32 lanes
+    per nonzero, one or two nonzeros in flight per group) and order, against
+    an FP64 evaluation; nnz not a multiple of a warp's share, so the last pass
+    is partial."""
+    import torch
+    dims = tuple([60, 50, 40, 30, 20][:N])
+    nnz = min(4099, int(np.prod(dims)) // 2)  # 1,500 for the 2-mode case
+    inds, vals = synth.uniform_tensor(dims, nnz, seed=10 * N + R)
+    nnz = vals.size
+    rng = np.random.default_rng(R)
+    stride = ((R - 1) // 8 + 1) * 8
+    facs = []
+    for d in dims:
+        a = np.zeros((d, stride), np.float32)
+        a[:, :R] = rng.standard_normal((d, R)).astype(np.float32)
+        facs.append(a)
+    dt = DeviceTensor.from_coo(COOTensor(dims, inds, vals))
+    got = dt.kruskal_values([torch.from_numpy(a).to(cuda) for a in facs], rank=R).cpu().numpy()
+    model = np.ones((nnz, R))
+    for a, ix in zip(facs, inds):
+        model *= a[ix, :R].astype(np.float64)
+    want = model.sum(1)
+    assert rel_err(got, want) < 1e-5
+    dt.free()
