@@ -1070,6 +1070,10 @@ int prepare_mode(ptiB200Tensor *t, uint32_t mode, cudaStream_t s, const Arrivals
 #ifndef PTI_COO_U
 #define PTI_COO_U 3
 #endif
+// ... and for 33 <= R <= 64 (3 fit the same 64-register budget as 2)
+#ifndef PTI_COO_U64
+#define PTI_COO_U64 3
+#endif
 #ifndef PTI_COO_MINB
 #define PTI_COO_MINB 4
 #endif
@@ -1166,7 +1170,7 @@ static int launch_r(bool hicoo, bool wide, const SchedArgs &a, const uint32_t *r
     if (R <= 8) return launch_coo<2, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
     if (R <= 16) return launch_coo<4, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
     if (R <= 32) return launch_coo<8, 4, PTI_COO_U, FT, NIN>(a, recs, ntiles, s);
-    if (R <= 64) return launch_coo<16, 4, 2, FT, NIN>(a, recs, ntiles, s);
+    if (R <= 64) return launch_coo<16, 4, PTI_COO_U64, FT, NIN>(a, recs, ntiles, s);
     return launch_coo<32, 4, 2, FT, NIN>(a, recs, ntiles, s);
 }
 
