@@ -6,8 +6,12 @@
 // are recomputed by the MTTKRP kernels rather than stored per nonzero.
 #include "kutil.cuh"
 #include "tensor.cuh"
+#include "tma.cuh"
 
 namespace pti {
+
+uint32_t *err_word(ptiB200Tensor *t);
+int ensure_err_word(ptiB200Tensor *t, cudaStream_t s);
 
 struct KVArgs {
     uint64_t nnz;
@@ -78,6 +82,123 @@ __global__ void __launch_bounds__(256) kruskal_values_kernel(KVArgs a)
     }
 }
 
+// The CP model over the mode-0 COO schedule of a 2- or 3-mode tensor (the
+// schedule the residual MTTKRPs walk): records {mode-0 row, other rows,
+// value} sorted by the mode-0 row, bulk-copied a tile at a time.  Runs of one
+// mode-0 row keep that factor row in registers, so a nonzero gathers the
+// other modes' rows only (2 instead of 3 for a 3-mode tensor).  Each value is
+// written to its input position (the schedule's permutation).
+constexpr uint32_t kKsTile = 2048;  // records per CTA
+#ifndef PTI_KS_U
+#define PTI_KS_U 3
+#endif
+// records in flight per lane group: 3 (64 registers, 4 CTAs per SM) measured
+// a little faster than 2 (48 registers, 5 CTAs) on a 20M-nonzero tensor
+constexpr int kKsU = PTI_KS_U;
+
+struct KSArgs {
+    uint64_t nnz;
+    uint32_t R, stride;
+    const uint32_t *recs;  // 4 words per record
+    const uint32_t *perm;  // schedule position -> input nonzero
+    const float *mats[3];
+    float *out;
+    uint32_t *err;
+};
+
+template <int G, int NIN>
+__global__ void __launch_bounds__(256) kruskal_sched_kernel(KSArgs a)
+{
+    static_assert(NIN == 1 || NIN == 2, "records of 4 words hold up to 3 modes");
+    __shared__ __align__(128) uint4 s_rec[kKsTile];
+    __shared__ uint64_t mbar;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t z0 = (uint64_t)blockIdx.x * kKsTile;
+    const uint32_t n = (uint32_t)((a.nnz - z0) < kKsTile ? (a.nnz - z0) : kKsTile);
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&mbar, 16 * n);
+        bulk_g2s_ef(s_rec, a.recs + z0 * 4, 16 * n, &mbar);
+    }
+    const bool ok = mbar_wait_bounded(&mbar, 0);
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) {
+            atomicOr(a.err, 2u);
+            mbar_wait_bounded(&mbar, 0);  // the copy lands before the CTA's shared memory is released
+        }
+        return;
+    }
+    constexpr uint32_t kGroups = 256 / G;
+    const uint32_t g = tid / G, lane = tid % G;
+    // the same slice length for every group, so the warp's groups run the
+    // same number of passes (the shuffles below need every lane)
+    const uint32_t per = (n + kGroups - 1) / kGroups;
+    const uint32_t j0 = min(g * per, n), j1 = min(j0 + per, n);
+    const uint32_t col = lane * 4;
+    const bool active = col < a.R;
+    const uint32_t c0 = active ? col : 0u;  // inactive lanes read column 0 and are masked
+    uint32_t cur = 0xFFFFFFFFu;
+    float4 arow = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t t = 0; t < per; t += kKsU) {
+        uint4 r[kKsU];
+        bool valid[kKsU];
+#pragma unroll
+        for (int u = 0; u < kKsU; ++u) {
+            const uint32_t j = j0 + t + u;
+            valid[u] = j < j1;
+            r[u] = valid[u] ? s_rec[j] : make_uint4(0u, 0u, 0u, 0u);
+        }
+        float4 f[kKsU][NIN];
+#pragma unroll
+        for (int u = 0; u < kKsU; ++u) {
+            const uint32_t rows[2] = {r[u].y, r[u].z};
+#pragma unroll
+            for (int k = 0; k < NIN; ++k) f[u][k] = load4(a.mats[1 + k] + (size_t)rows[k] * a.stride, c0);
+        }
+        // the mode-0 rows: the cached row while every record of the warp's
+        // batch continues it, else one gather per record
+        bool same = true;
+#pragma unroll
+        for (int u = 0; u < kKsU; ++u) same = same && (!valid[u] || r[u].x == cur);
+        float4 fa[kKsU];
+        if (__all_sync(0xffffffffu, same)) {
+#pragma unroll
+            for (int u = 0; u < kKsU; ++u) fa[u] = arow;
+        } else {
+#pragma unroll
+            for (int u = 0; u < kKsU; ++u) fa[u] = load4(a.mats[0] + (size_t)r[u].x * a.stride, c0);
+#pragma unroll
+            for (int u = 0; u < kKsU; ++u)
+                if (valid[u]) {
+                    cur = r[u].x;
+                    arow = fa[u];
+                }
+        }
+        float s[kKsU];
+#pragma unroll
+        for (int u = 0; u < kKsU; ++u) {
+            float4 p = fa[u];
+#pragma unroll
+            for (int k = 0; k < NIN; ++k) p = mul4(p, f[u][k]);
+            p = mask4(p, col, a.R);
+            s[u] = (p.x + p.y) + (p.z + p.w);
+        }
+#pragma unroll
+        for (int u = 0; u < kKsU; ++u)
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o, G);
+        if (lane == 0) {
+#pragma unroll
+            for (int u = 0; u < kKsU; ++u)
+                if (valid[u]) a.out[__ldg(a.perm + z0 + j0 + t + u)] = s[u];
+        }
+    }
+}
+
 #ifndef PTI_KV_U
 #define PTI_KV_U 2
 #endif
@@ -96,6 +217,20 @@ static int lanes_for(uint32_t R)
     int g = 1;
     while ((uint32_t)g < q && g < 32) g *= 2;
     return g;
+}
+
+template <int NIN>
+static int launch_ks(int G, const KSArgs &a, unsigned tiles, cudaStream_t s)
+{
+    switch (G) {
+        case 1: kruskal_sched_kernel<1, NIN><<<tiles, 256, 0, s>>>(a); break;
+        case 2: kruskal_sched_kernel<2, NIN><<<tiles, 256, 0, s>>>(a); break;
+        case 4: kruskal_sched_kernel<4, NIN><<<tiles, 256, 0, s>>>(a); break;
+        case 8: kruskal_sched_kernel<8, NIN><<<tiles, 256, 0, s>>>(a); break;
+        case 16: kruskal_sched_kernel<16, NIN><<<tiles, 256, 0, s>>>(a); break;
+        default: kruskal_sched_kernel<32, NIN><<<tiles, 256, 0, s>>>(a); break;
+    }
+    return 0;
 }
 
 template <int NM>
@@ -141,6 +276,26 @@ int ptiB200KruskalValues(ptiB200Tensor *t, const float *const *dev_factors, ptiI
     }
     a.out = dev_out;
     const int G = lanes_for(rank);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // 2- and 3-mode tensors up to rank 128: over the mode-0 schedule (built
+    // here if no MTTKRP has built it yet)
+    if ((t->nmodes == 2 || t->nmodes == 3) && rank <= 128 && t->nnz < 0xFFFFFFFFull) {
+        PTI_TRY(prepare_mode(t, 0, st));
+        PTI_TRY(ensure_err_word(t, st));
+        KSArgs k{};
+        k.nnz = t->nnz;
+        k.R = rank;
+        k.stride = stride;
+        k.recs = t->coo_plan[0].recs.as<uint32_t>();
+        k.perm = t->coo_plan[0].perm.as<uint32_t>();
+        for (uint32_t m = 0; m < t->nmodes; ++m) k.mats[m] = dev_factors[m];
+        k.out = dev_out;
+        k.err = err_word(t);
+        const unsigned tiles = (unsigned)((t->nnz + kKsTile - 1) / kKsTile);
+        PTI_TRY(t->nmodes == 3 ? launch_ks<2>(G, k, tiles, st) : launch_ks<1>(G, k, tiles, st));
+        PTI_CUDA(cudaGetLastError(), mod);
+        return 0;
+    }
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((t->nnz * G + 255) / 256, (uint64_t)sm_count() * 16));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
