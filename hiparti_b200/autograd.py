@@ -31,13 +31,38 @@ class CPValues(torch.autograd.Function):
     def backward(ctx, grad_model):
         factors = ctx.saved_tensors
         g = grad_model.contiguous().to(torch.float32)
+        # the per-mode MTTKRPs are independent: each runs on a stream of its
+        # own, so one mode's residual gather overlaps another mode's walk
+        cur = torch.cuda.current_stream()
+        streams = _side_streams(g.device, len(factors))
         grads = []
-        for k in range(len(factors)):
+        for k, s in enumerate(streams):
             if ctx.needs_input_grad[2 + k]:
-                grads.append(ctx.dt.mttkrp_values(g, list(factors), k, rank=ctx.rank))
+                s.wait_stream(cur)
+                with torch.cuda.stream(s):
+                    grads.append(ctx.dt.mttkrp_values(g, list(factors), k, rank=ctx.rank))
+                g.record_stream(s)
+                for f in factors:
+                    f.record_stream(s)
             else:
                 grads.append(None)
+        for k, s in enumerate(streams):
+            if grads[k] is not None:
+                cur.wait_stream(s)
+                grads[k].record_stream(cur)
         return (None, None, *grads)
+
+
+_STREAMS = {}
+
+
+def _side_streams(device, n):
+    """n CUDA streams of `device`, made once and reused."""
+    key = (device.index if device.index is not None else torch.cuda.current_device(), n)
+    if key not in _STREAMS:
+        with torch.cuda.device(key[0]):
+            _STREAMS[key] = [torch.cuda.Stream() for _ in range(n)]
+    return _STREAMS[key]
 
 
 def cp_values(dt: DeviceTensor, factors, rank=None):
